@@ -1,0 +1,68 @@
+#!/usr/bin/env python3
+"""Build the golden fixtures of the parity tests from axtb's reference matrix.
+
+axtb records, for every case of its reference matrix, the inputs (generated by the numpy
+builders in ``tests/reference_matrix/{cases,structures}.py``) and the results of axtb 0.1.0
+in its default conventions (``tests/reference_matrix/results.json``: ``programs.axtb`` with the
+energy, the energy terms, Mulliken charges, dipole and SCF iterations, at SCF accuracy 1e-6).
+This script re-runs the builders (plain numpy, importable without axtb itself), keeps the
+gas-phase cases with dispersion that the GFN2 E+grad path covers (categories elements,
+structures, multielement, charges, spin, etemp_acc, open_shell_metals, threads) and writes
+
+    tests/golden/reference_matrix.json
+
+with numbers, positions (bohr), charge, uhf, accuracy, etemp, max_iter and the recorded axtb
+results. Run once in a checkout that has the axtb sources::
+
+    python tests/golden/make_golden.py [path-to-axtb-checkout]
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+OUT = Path(__file__).with_name("reference_matrix.json")
+KEEP = {"elements", "structures", "multielement", "charges", "spin", "etemp_acc", "open_shell_metals", "threads"}
+
+
+def main() -> None:
+    sys.path.insert(0, str(REF / "tests" / "reference_matrix"))
+    import cases as C  # noqa: E402  (axtb's numpy case builders)
+
+    results = json.loads((REF / "tests" / "reference_matrix" / "results.json").read_text())["cases"]
+    out = []
+    for name in sorted(KEEP):
+        for c in C.CATEGORIES[name]():
+            r = results.get(c["id"])
+            if r is None:
+                continue
+            ax = r.get("programs", {}).get("axtb")
+            if not ax or not ax.get("ok") or "energy" not in ax:
+                continue
+            if any(k in c for k in ("alpb", "gbsa", "solvation_state")) or c.get("dispersion") is False:
+                continue
+            out.append({
+                "id": c["id"],
+                "category": name,
+                "numbers": c["numbers"],
+                "positions": c["positions"],
+                "charge": c["charge"],
+                "uhf": c["uhf"],
+                "accuracy": c.get("accuracy", 1.0),
+                "etemp": c.get("etemp", 300.0),
+                "max_iter": c.get("max_iter", 250),
+                "energy": ax["energy"],
+                "terms": ax.get("terms"),
+                "charges": ax.get("charges"),
+                "dipole": ax.get("dipole"),
+                "iterations": ax.get("iterations"),
+            })
+    OUT.write_text(json.dumps({"source": "axtb tests/reference_matrix/results.json (programs.axtb)",
+                               "cases": out}, indent=0))
+    print(f"wrote {len(out)} cases to {OUT}")
+
+
+if __name__ == "__main__":
+    main()
