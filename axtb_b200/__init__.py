@@ -1,0 +1,7 @@
+"""B200-native GFN2-xTB energy + analytic gradient (the single point of axtb's calculator).
+
+``Calculator`` and ``Batch`` (axtb_b200.calculator) drive the sm_100a engine in
+``libaxtb_gpu.so`` through its C ABI (include/axtb_gpu.h); ``structures`` builds the synthetic
+workloads; ``autograd`` exposes the batched energy to PyTorch.
+"""
+from .calculator import AxtbError, Batch, Calculator, SinglePoint, basis_size  # noqa: F401

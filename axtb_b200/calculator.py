@@ -1,0 +1,223 @@
+"""Python face of the engine, mirroring axtb's calculator interface.
+
+``Calculator(numbers, positions, charge=0, uhf=None, **options)`` is the counterpart of
+``axtb::Calculator::new(Hamiltonian::Gfn2, numbers, positions, charge, uhf, Options)``
+(crates/axtb/src/calculator.rs:92-128) and ``Calculator.singlepoint(positions, gradient=True)``
+of ``Method::singlepoint`` (crates/base/src/method/mod.rs:62), returning the fields of
+``SinglePoint`` (crates/base/src/method/results.rs:39-57). Errors raise ``AxtbError`` with the
+kind of crates/base/src/error.rs:8-24. ``Batch`` runs many molecules in one device pass.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+
+KINDS = {1: "input", 2: "unsupported_element", 3: "scf_not_converged", 4: "numerical", 5: "device"}
+TERM_NAMES = ("repulsion", "dispersion", "electronic", "isotropic_es", "third_order", "anisotropic", "entropy",
+              "band")
+
+
+class AxtbError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{KINDS.get(code, 'error')}: {message}")
+        self.code = code
+        self.kind = KINDS.get(code, "error")
+
+
+@dataclass
+class SinglePoint:
+    energy: float
+    gradient: np.ndarray | None
+    charges: np.ndarray
+    dipole: np.ndarray
+    qsh: np.ndarray
+    dpat: np.ndarray
+    qpat: np.ndarray
+    terms: dict = field(default_factory=dict)
+    iterations: int = 0
+    converged: bool = False
+    status: int = 0
+    energy_change: float = 0.0
+    residual: float = 0.0
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def basis_size(numbers):
+    z = np.ascontiguousarray(numbers, dtype=np.int32)
+    nsh, nao = C.c_int32(), C.c_int32()
+    rc = _lib.load().axtb_gpu_basis_size(z.ctypes.data_as(C.POINTER(C.c_int32)), len(z), C.byref(nsh), C.byref(nao))
+    if rc != 0:
+        raise AxtbError(rc, "unsupported element")
+    return nsh.value, nao.value
+
+
+class _ResultBuffers:
+    def __init__(self, nat, nsh):
+        self.grad = np.zeros((nat, 3))
+        self.q = np.zeros(nat)
+        self.dip = np.zeros(3)
+        self.qsh = np.zeros(nsh)
+        self.dp = np.zeros((nat, 3))
+        self.qp = np.zeros((nat, 6))
+        self.res = _lib.AxtbResult()
+        r = self.res
+        r.gradient, r.charges, r.dipole = _ptr(self.grad), _ptr(self.q), _ptr(self.dip)
+        r.qsh, r.dpat, r.qpat = _ptr(self.qsh), _ptr(self.dp), _ptr(self.qp)
+
+    def result(self, gradient: bool) -> SinglePoint:
+        r = self.res
+        return SinglePoint(energy=r.energy, gradient=self.grad.copy() if gradient else None, charges=self.q.copy(),
+                           dipole=self.dip.copy(), qsh=self.qsh.copy(), dpat=self.dp.copy(), qpat=self.qp.copy(),
+                           terms=dict(zip(TERM_NAMES, list(r.terms))), iterations=r.iterations,
+                           converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
+                           residual=r.residual)
+
+
+def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0):
+    return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
+                                damping=float(damping), guess=0 if guess == "eeq" else 1,
+                                precision=0 if precision == "fp64" else 1, device=int(device))
+
+
+class Calculator:
+    """GFN2-xTB calculator of one molecule on the GPU (axtb::Calculator)."""
+
+    def __init__(self, numbers, positions=None, charge=0.0, uhf=None, **options):
+        lib = _lib.load()
+        self.numbers = np.ascontiguousarray(numbers, dtype=np.int32)
+        self.nat = len(self.numbers)
+        self.nsh, self.nao = basis_size(self.numbers)
+        self._opts = _options(**options)
+        h = C.c_void_p()
+        rc = lib.axtb_gpu_create(self.numbers.ctypes.data_as(C.POINTER(C.c_int32)), self.nat, float(charge),
+                                 -1 if uhf is None else int(uhf), C.byref(self._opts), C.byref(h))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        self._h = h
+        self._buf = _ResultBuffers(self.nat, self.nsh)
+        self.positions = None if positions is None else np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+
+    def singlepoint(self, positions=None, gradient=True) -> SinglePoint:
+        x = self.positions if positions is None else np.asarray(positions, dtype=np.float64).reshape(-1, 3)
+        x = np.ascontiguousarray(x)
+        rc = _lib.load().axtb_gpu_singlepoint(self._h, _ptr(x), int(bool(gradient)), C.byref(self._buf.res))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(self._h))
+        return self._buf.result(gradient)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().axtb_gpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many molecules (numbers, positions, charge, uhf) in one device pass."""
+
+    def __init__(self, molecules, **options):
+        lib = _lib.load()
+        self._keep = []
+        self.mols = []
+        arr = (_lib.AxtbMol * len(molecules))()
+        for i, m in enumerate(molecules):
+            z = np.ascontiguousarray(m[0], dtype=np.int32)
+            x = np.ascontiguousarray(m[1], dtype=np.float64).reshape(-1, 3)
+            q = float(m[2]) if len(m) > 2 else 0.0
+            u = m[3] if len(m) > 3 else None
+            self._keep += [z, x]
+            arr[i].nat = len(z)
+            arr[i].numbers = z.ctypes.data_as(C.POINTER(C.c_int32))
+            arr[i].positions = _ptr(x)
+            arr[i].charge = q
+            arr[i].uhf = -1 if u is None else int(u)
+            self.mols.append((z, x))
+        self._opts = _options(**options)
+        b = C.c_void_p()
+        rc = lib.axtb_gpu_batch_create(arr, len(molecules), C.byref(self._opts), C.byref(b))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        self._b = b
+        self.nmol = len(molecules)
+        self.natoms = np.array([len(z) for z, _ in self.mols])
+        self._bufs = [_ResultBuffers(len(z), basis_size(z)[0]) for z, _ in self.mols]
+        self._res = (_lib.AxtbResult * self.nmol)()
+
+    def run(self, positions=None, gradient=True):
+        """Single points of every molecule (positions: list of (nat, 3) arrays or None for the
+        set-up geometries); returns a list of SinglePoint (status per molecule)."""
+        lib = _lib.load()
+        for i, bf in enumerate(self._bufs):
+            self._res[i] = bf.res
+        st = np.zeros(self.nmol, dtype=np.int32)
+        xp = None
+        if positions is not None:
+            flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1) for p in positions]))
+            xp = _ptr(flat)
+        rc = lib.axtb_gpu_batch_run(self._b, xp, int(bool(gradient)), self._res, st.ctypes.data_as(C.POINTER(C.c_int32)))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        out = []
+        for i, bf in enumerate(self._bufs):
+            bf.res = self._res[i]
+            out.append(bf.result(gradient))
+        return out
+
+    def run_device(self, d_positions: int, d_energy: int, d_gradient: int, gradient=True):
+        """Device-resident run: pointers (ints) to device arrays of positions (natT*3), energies
+        (nmol) and gradients (natT*3). Returns the per-molecule status array."""
+        st = np.zeros(self.nmol, dtype=np.int32)
+        rc = _lib.load().axtb_gpu_batch_run_device(self._b, C.c_void_p(d_positions), int(bool(gradient)),
+                                                   C.c_void_p(d_energy), C.c_void_p(d_gradient),
+                                                   st.ctypes.data_as(C.POINTER(C.c_int32)))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        return st
+
+    @property
+    def stream(self) -> int:
+        return _lib.load().axtb_gpu_batch_stream(self._b) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(_lib.load().axtb_gpu_batch_launches(self._b))
+
+    def debug(self, mol: int, what: str) -> np.ndarray:
+        z, _ = self.mols[mol]
+        nat = len(z)
+        nsh, nao = basis_size(z)
+        size = {"cn": nat, "eeq": nat, "emo": nao, "focc": nao, "dipole": 3 * nao * nao,
+                "quadrupole": 6 * nao * nao}.get(what, nao * nao)
+        out = np.zeros(size)
+        rc = _lib.load().axtb_gpu_batch_debug(self._b, mol, _lib.DBG[what], _ptr(out))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        if what in ("dipole", "quadrupole"):
+            k = 3 if what == "dipole" else 6
+            return out.reshape(k, nao, nao).transpose(0, 2, 1).copy()
+        if size == nao * nao and what not in ("cn", "eeq", "emo", "focc"):
+            return out.reshape(nao, nao).T.copy()
+        return out
+
+    def close(self):
+        if getattr(self, "_b", None):
+            _lib.load().axtb_gpu_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,878 @@
+// B200 (sm_100a) GFN2-xTB energy + gradient engine behind the C ABI of include/axtb_gpu.h.
+//
+// Host side: validation and model set-up of every molecule (basis from the STO-nG tables,
+// H0/ES/AES/D4/repulsion parameters, electron counts; crates/axtb/src/gfn2.rs:34-133,
+// crates/axtb/src/basis.rs:20-229, crates/base/src/molecule.rs:35-99, crates/axtb/src/xtb.rs:1159-1212),
+// the flat device layout of a batch, and the SCF driver (crates/axtb/src/scf/driver.rs:180-299,
+// crates/axtb/src/xtb.rs:437-861). Device side: the kernels of k_geometry.cuh, k_integrals.cuh,
+// k_scf.cuh and team_kernel.cuh. Single translation unit, so every kernel is in this library.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/axtb_gpu.h"
+#include "common.cuh"
+#include "k_geometry.cuh"
+#include "k_integrals.cuh"
+#include "k_scf.cuh"
+#include "params/gfn2_tables.h"
+#include "team_kernel.cuh"
+
+using std::vector;
+
+namespace {
+
+// ------------------------------------------------------------------ constants (crates/base/src/units.rs)
+const double PI_ = 3.14159265358979323846;
+const double AATOAU = 1.0 / (5.29177210544e-11 * 1e10);
+const double KB_HARTREE = 3.1668115634564e-6;
+const double MCTC_AATOAU =
+    1.0 / ((6.62607015e-34 / (2.0 * PI_)) / (9.1093837015e-31 * 299792458.0 * 7.2973525693e-3) * 1e10);
+const double ATOMIC_RAD_AA[86] = {
+    0.32, 0.37, 1.30, 0.99, 0.84, 0.75, 0.71, 0.64, 0.60, 0.62, 1.60, 1.40, 1.24, 1.14, 1.09, 1.04, 1.00,
+    1.01, 2.00, 1.74, 1.59, 1.48, 1.44, 1.30, 1.29, 1.24, 1.18, 1.17, 1.22, 1.20, 1.23, 1.20, 1.20, 1.18,
+    1.17, 1.16, 2.15, 1.90, 1.76, 1.64, 1.56, 1.46, 1.38, 1.36, 1.34, 1.30, 1.36, 1.40, 1.42, 1.40, 1.40,
+    1.37, 1.36, 1.36, 2.38, 2.06, 1.94, 1.84, 1.90, 1.88, 1.86, 1.85, 1.83, 1.82, 1.81, 1.80, 1.79, 1.77,
+    1.77, 1.78, 1.74, 1.64, 1.58, 1.50, 1.41, 1.36, 1.32, 1.30, 1.30, 1.32, 1.44, 1.45, 1.50, 1.42, 1.48, 1.46};
+const double FREQ[23] = {0.000001, 0.050000, 0.100000, 0.200000, 0.300000, 0.400000, 0.500000, 0.600000,
+                         0.700000, 0.800000, 0.900000, 1.000000, 1.200000, 1.400000, 1.600000, 1.800000,
+                         2.000000, 2.500000, 3.000000, 4.000000, 5.000000, 7.500000, 10.00000};
+
+thread_local std::string g_last_error;
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CK(x)                                                                                   \
+    do {                                                                                        \
+        cudaError_t err__ = (x);                                                                \
+        if (err__ != cudaSuccess) throw Fail(AXTB_ERR_DEVICE, std::string("CUDA: ") + cudaGetErrorString(err__) + " at " #x); \
+    } while (0)
+
+// ------------------------------------------------------------------ host model of one molecule
+struct HShell {
+    int l, np, z, ish;
+    double a[6], c[6], amin;
+};
+
+HShell sto_shell(int z, int ish) {
+    using namespace gfn2tab;
+    int ng = NUMBER_OF_PRIMITIVES[z - 1][ish], n = PRINCIPAL_QUANTUM_NUMBER[z - 1][ish], l = ANG_SHELL[z - 1][ish];
+    double zeta = SLATER_EXPONENT[z - 1][ish];
+    int ityp = (l == 0 ? n : l == 1 ? 4 + n : 7 + n) - 1;
+    HShell s{};
+    s.l = l;
+    s.np = ng;
+    s.z = z;
+    s.ish = ish;
+    double z2 = zeta * zeta;
+    auto fill = [&](const double* a, const double* c) {
+        for (int i = 0; i < ng; i++) {
+            s.a[i] = a[i] * z2;
+            s.c[i] = c[i];
+        }
+    };
+    switch (ng) {
+        case 1: s.a[0] = P_ALPHA1[ityp] * z2; s.c[0] = 1.0; break;
+        case 2: fill(P_ALPHA2[ityp], P_COEFF2[ityp]); break;
+        case 3: fill(P_ALPHA3[ityp], P_COEFF3[ityp]); break;
+        case 4: fill(P_ALPHA4[ityp], P_COEFF4[ityp]); break;
+        case 5: fill(P_ALPHA5[ityp], P_COEFF5[ityp]); break;
+        case 6:
+            if (n == 6) fill(l == 0 ? P_ALPHA_6S : P_ALPHA_6P, l == 0 ? P_COEFF_6S : P_COEFF_6P);
+            else fill(P_ALPHA6[ityp], P_COEFF6[ityp]);
+            break;
+        default: throw Fail(AXTB_ERR_INPUT, "STO-NG: unsupported primitive count");
+    }
+    const double DF[3] = {1.0, 1.0, 3.0};
+    s.amin = INFINITY;
+    for (int i = 0; i < ng; i++) {
+        double r = std::sqrt(4.0 * s.a[i]), pw = 1.0;
+        for (int k = 0; k < l; k++) pw *= r;
+        s.c[i] *= std::pow(2.0 / PI_ * s.a[i], 0.75) * pw / std::sqrt(DF[l]);
+        s.amin = std::min(s.amin, s.a[i]);
+    }
+    return s;
+}
+
+double rcov_codata(int z) { return 4.0 / 3.0 * (gfn2tab::COVALENT_RAD_2009_AA[z - 1] * AATOAU); }
+double rcov_mctc(int z) { return 4.0 / 3.0 * (MCTC_AATOAU * gfn2tab::COVALENT_RAD_2009_AA[z - 1]); }
+
+struct HostMol {
+    int nat = 0;
+    vector<int> Z;
+    vector<double> xyz;
+    double charge = 0.0;
+    int uhf = -1;
+    double nalpha = 0, nbeta = 0;
+    int nsh = 0, nao = 0;
+};
+
+// validation (crates/base/src/molecule.rs:35-99) and electrons (crates/axtb/src/xtb.rs:1178-1212)
+void check_molecule(HostMol& m) {
+    using namespace gfn2tab;
+    if (m.nat <= 0) throw Fail(AXTB_ERR_INPUT, "molecule has no atoms");
+    for (int z : m.Z) {
+        if (z <= 0 || z > 118) throw Fail(AXTB_ERR_INPUT, "invalid atomic number " + std::to_string(z));
+        if (z > 86) throw Fail(AXTB_ERR_UNSUPPORTED_ELEMENT, "GFN2-xTB: unsupported element Z=" + std::to_string(z));
+    }
+    if (!std::isfinite(m.charge)) throw Fail(AXTB_ERR_INPUT, "the charge must be a finite number");
+    for (double v : m.xyz)
+        if (!std::isfinite(v)) throw Fail(AXTB_ERR_INPUT, "a position is not finite");
+    vector<int> ord(m.nat);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return m.xyz[3 * a] < m.xyz[3 * b]; });
+    for (int k = 0; k < m.nat; k++)
+        for (int q = k + 1; q < m.nat; q++) {
+            int i = ord[k], j = ord[q];
+            if (m.xyz[3 * j] - m.xyz[3 * i] >= 0.1) break;
+            double d2 = 0;
+            for (int c = 0; c < 3; c++) d2 += (m.xyz[3 * i + c] - m.xyz[3 * j + c]) * (m.xyz[3 * i + c] - m.xyz[3 * j + c]);
+            if (std::sqrt(d2) < 0.1)
+                throw Fail(AXTB_ERR_INPUT, "atoms " + std::to_string(std::min(i, j) + 1) + " and " +
+                                               std::to_string(std::max(i, j) + 1) + " are closer than 0.1 bohr");
+        }
+    if (m.charge != std::floor(m.charge)) throw Fail(AXTB_ERR_INPUT, "the charge must be an integer");
+    double nref = 0.0;
+    m.nsh = m.nao = 0;
+    for (int z : m.Z)
+        for (int ish = 0; ish < NSHELL[z - 1]; ish++) {
+            nref += REFERENCE_OCC[z - 1][ANG_SHELL[z - 1][ish]];
+            m.nsh++;
+            m.nao += 2 * ANG_SHELL[z - 1][ish] + 1;
+        }
+    double nocc = nref - m.charge;
+    long nel = std::lround(nocc);
+    long par = ((nel % 2) + 2) % 2;
+    long nuhf = par;
+    if (m.uhf >= 0) {
+        if ((m.uhf % 2) != par) throw Fail(AXTB_ERR_INPUT, "electron count and unpaired electrons are not compatible");
+        nuhf = m.uhf;
+    }
+    if (nocc < 0.0) throw Fail(AXTB_ERR_INPUT, "the charge leaves a negative electron count");
+    if (nuhf > nocc) throw Fail(AXTB_ERR_INPUT, "more unpaired electrons than electrons");
+    m.nalpha = (nocc + nuhf) / 2.0;
+    m.nbeta = (nocc - nuhf) / 2.0;
+    if (m.nalpha > m.nao + 1e-9) throw Fail(AXTB_ERR_INPUT, "too many electrons for the basis");
+}
+
+struct Opt {
+    double acc = 1.0, etemp = 300.0, damping = 0.4;
+    int max_iter = 250, guess = 0, precision = 0, device = 0;
+};
+
+void check_options(const Opt& o) {
+    if (!(o.acc > 0.0 && std::isfinite(o.acc))) throw Fail(AXTB_ERR_INPUT, "SCF accuracy must be a positive number");
+    if (!(o.etemp >= 0.0 && std::isfinite(o.etemp))) throw Fail(AXTB_ERR_INPUT, "electronic temperature must be >= 0 K");
+    if (!(o.damping > 0.0 && o.damping <= 1.0)) throw Fail(AXTB_ERR_INPUT, "SCF damping must be in (0, 1]");
+    if (o.max_iter <= 0) throw Fail(AXTB_ERR_INPUT, "the SCF needs at least 1 iteration");
+}
+
+// ------------------------------------------------------------------ device arena
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+    template <class T>
+    T* take(size_t n) {
+        size_t bytes = ((n * sizeof(T)) + 255) & ~size_t(255);
+        if (used + bytes > size) throw Fail(AXTB_ERR_DEVICE, "device arena exhausted");
+        T* p = reinterpret_cast<T*>(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+template <class T>
+size_t padded(size_t n) {
+    return ((n * sizeof(T)) + 255) & ~size_t(255);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the batch engine
+struct AxtbBatch {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    Opt opt;
+    vector<HostMol> mols;
+    int nmol = 0, natT = 0, nshT = 0, naoT = 0;
+    long long nnT = 0, npairT = 0, npdT = 0, nvecT = 0, nsqT = 0, ntiles = 0, nwk = 0, nhist = 0;
+    int hist_cap = 0, nsp = 0;
+    axg::Batch B{};
+    axg::State S{};
+    axg::TeamPlan P{};
+    void* dmem = nullptr;
+    void* hpin = nullptr;  // pinned staging
+    size_t hpin_size = 0;
+    long long *d_pair0 = nullptr, *d_pd0 = nullptr, *d_tile0 = nullptr, *d_sq0 = nullptr;
+    double *d_wt = nullptr, *d_tt = nullptr, *d_eatm = nullptr;
+    int grid = 0;
+    int64_t launches = 0;
+    // host copies of the per-molecule offsets
+    vector<long long> m_mat0, m_pair0, m_vec0;
+    vector<int> m_at0, m_sh0, m_ao0;
+    vector<double> e_rep, e_atm;
+    std::string err;
+
+    void build(const vector<HostMol>& in, const Opt& o);
+    void run(bool want_grad, bool warm = false);
+    void extract(AxtbResult* outs, int32_t* status, bool want_grad);
+    void upload_positions(const double* host_xyz, bool device_ptr);
+    ~AxtbBatch();
+};
+
+AxtbBatch::~AxtbBatch() {
+    if (dmem) cudaFree(dmem);
+    if (hpin) cudaFreeHost(hpin);
+    if (st) cudaStreamDestroy(st);
+}
+
+void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
+    using namespace gfn2tab;
+    opt = o;
+    mols = in;
+    nmol = (int)mols.size();
+    if (nmol <= 0) throw Fail(AXTB_ERR_INPUT, "empty batch");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        throw Fail(AXTB_ERR_DEVICE, "no CUDA device: the GFN2-xTB engine has no CPU path");
+    device = o.device;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    // ---- host layout
+    vector<int> m_nat(nmol), m_nsh(nmol), m_nao(nmol), m_dim(nmol);
+    vector<long long> m_hist0(nmol), m_pd0(nmol), m_tile0(nmol), m_wk0(nmol), m_sq0(nmol);
+    vector<double> m_na(nmol), m_nb(nmol), m_ch(nmol);
+    m_at0.resize(nmol);
+    m_sh0.resize(nmol);
+    m_ao0.resize(nmol);
+    m_mat0.resize(nmol);
+    m_pair0.resize(nmol);
+    m_vec0.resize(nmol);
+    hist_cap = std::min(o.max_iter, nmol > 16 ? 64 : 128);
+    const int MAXCH = 16;
+    natT = nshT = naoT = 0;
+    nnT = npairT = npdT = nvecT = nsqT = ntiles = nwk = nhist = 0;
+    for (int m = 0; m < nmol; m++) {
+        HostMol& h = mols[m];
+        m_nat[m] = h.nat;
+        m_nsh[m] = h.nsh;
+        m_nao[m] = h.nao;
+        m_dim[m] = h.nsh + 9 * h.nat;
+        m_at0[m] = natT;
+        m_sh0[m] = nshT;
+        m_ao0[m] = naoT;
+        m_mat0[m] = nnT;
+        m_pair0[m] = npairT;
+        m_pd0[m] = npdT;
+        m_vec0[m] = nvecT;
+        m_hist0[m] = nhist;
+        m_sq0[m] = nsqT;
+        m_tile0[m] = ntiles;
+        m_wk0[m] = nwk;
+        m_na[m] = h.nalpha;
+        m_nb[m] = h.nbeta;
+        m_ch[m] = h.charge;
+        long long n = h.nao;
+        natT += h.nat;
+        nshT += h.nsh;
+        naoT += h.nao;
+        nnT += (std::max(n * n, 64LL * 64LL) + 31) & ~31LL;  // 256-byte aligned planes
+        npairT += (long long)h.nat * (h.nat - 1) / 2;
+        npdT += (long long)h.nat * (h.nat + 1) / 2;
+        nvecT += m_dim[m];
+        nhist += (long long)hist_cap * m_dim[m];
+        nsqT += (long long)h.nat * h.nat;
+        long long nt = (n + 31) / 32;
+        ntiles += nt * nt;
+        long long nw = std::max(n, 64LL);
+        nwk += (2 + MAXCH) * nw + 64LL * nw + 2 * 64 * 64 + 2 * 64LL * nw + 64LL * nw + 64;
+    }
+    // atoms / shells / AOs
+    vector<int> a_Z(natT), a_mol(natT), a_sh0(natT), a_nsh(natT), a_ao0(natT), a_sp(natT);
+    vector<double> a_rcov(natT), a_rad(natT), a_amin(natT), a_rcov_eeq(natT), a_en(natT), a_aes_rad(natT),
+        a_aes_vcn(natT), a_dk(natT), a_qk(natT), a_ra(natT), a_rz(natT), a_chi(natT), a_eta(natT), a_kcn(natT),
+        a_erad(natT);
+    vector<int> s_l(nshT), s_np(nshT), s_at(nshT), s_ao0(nshT), s_ish(nshT), s_mol(nshT), s_Z(nshT);
+    vector<double> s_alpha((size_t)nshT * 6, 0.0), s_coeff((size_t)nshT * 6, 0.0), s_amin(nshT), s_se0(nshT),
+        s_kcn(nshT), s_shpoly(nshT), s_refocc(nshT), s_hard(nshT), s_gam3(nshT), s_slater(nshT);
+    vector<int> o_sh(naoT), o_at(naoT);
+    vector<int> species;
+    const double SHD[3] = {1.0, 0.5, 0.25};
+    {
+        int ia = 0, is = 0, io = 0;
+        for (int m = 0; m < nmol; m++) {
+            const HostMol& h = mols[m];
+            for (int i = 0; i < h.nat; i++, ia++) {
+                int z = h.Z[i];
+                auto it = std::find(species.begin(), species.end(), z);
+                int sp = (int)(it - species.begin());
+                if (it == species.end()) species.push_back(z);
+                a_Z[ia] = z;
+                a_mol[ia] = m;
+                a_sh0[ia] = is;
+                a_nsh[ia] = NSHELL[z - 1];
+                a_ao0[ia] = io;
+                a_sp[ia] = sp;
+                a_rcov[ia] = rcov_codata(z);
+                a_rad[ia] = ATOMIC_RAD_AA[z - 1] * AATOAU;
+                a_rcov_eeq[ia] = rcov_mctc(z);
+                a_en[ia] = PAULING_EN[z - 1];
+                a_aes_rad[ia] = P_RAD[z - 1];
+                a_aes_vcn[ia] = P_VCN[z - 1];
+                a_dk[ia] = P_DKERNEL[z - 1];
+                a_qk[ia] = P_QKERNEL[z - 1];
+                a_ra[ia] = REP_ALPHA[z - 1];
+                a_rz[ia] = REP_ZEFF[z - 1];
+                if (z > 103) throw Fail(AXTB_ERR_UNSUPPORTED_ELEMENT, "EEQ: unsupported element");
+                a_chi[ia] = EEQ_CHI[z - 1];
+                a_eta[ia] = EEQ_ETA[z - 1];
+                a_kcn[ia] = EEQ_KCNCHI[z - 1];
+                a_erad[ia] = EEQ_RAD[z - 1];
+                double amin = INFINITY;
+                for (int ish = 0; ish < NSHELL[z - 1]; ish++, is++) {
+                    HShell sh = sto_shell(z, ish);
+                    int l = sh.l;
+                    s_l[is] = l;
+                    s_np[is] = sh.np;
+                    s_at[is] = ia;
+                    s_ao0[is] = io;
+                    s_ish[is] = ish;
+                    s_mol[is] = m;
+                    s_Z[is] = z;
+                    for (int p = 0; p < 6; p++) {
+                        s_alpha[(size_t)is * 6 + p] = sh.a[p];
+                        s_coeff[(size_t)is * 6 + p] = sh.c[p];
+                    }
+                    s_amin[is] = sh.amin;
+                    amin = std::min(amin, sh.amin);
+                    s_se0[is] = P_SELFENERGY[z - 1][ish];
+                    s_kcn[is] = P_KCN[z - 1][l];
+                    s_shpoly[is] = P_SHPOLY[z - 1][l];
+                    s_refocc[is] = REFERENCE_OCC[z - 1][l];
+                    s_hard[is] = HUBBARD_PARAMETER[z - 1] * SHELL_HUBBARD[z - 1][l];
+                    s_gam3[is] = P_HUBBARD_DERIVS[z - 1] * SHD[l];
+                    s_slater[is] = SLATER_EXPONENT[z - 1][ish];
+                    for (int k = 0; k < 2 * l + 1; k++, io++) {
+                        o_sh[io] = is;
+                        o_at[io] = ia;
+                    }
+                }
+                a_amin[ia] = amin;
+            }
+        }
+    }
+    // D4 species tables (crates/d4/src/model.rs:140-217, 319-386)
+    nsp = (int)species.size();
+    vector<int> sp_nref(nsp), sp_ngw((size_t)nsp * 7, 1);
+    vector<double> sp_refcn((size_t)nsp * 7, 0.0), sp_refq((size_t)nsp * 7, 0.0), sp_zeff(nsp), sp_gi(nsp),
+        sp_rcov(nsp), sp_en(nsp), sp_rr((size_t)nsp * nsp), sp_r0((size_t)nsp * nsp);
+    vector<double> aiw((size_t)nsp * 7 * 23, 0.0), c6ref((size_t)nsp * nsp * 49, 0.0), r4r2(nsp);
+    for (int sp = 0; sp < nsp; sp++) {
+        int z = species[sp], nr = REFN[z - 1];
+        sp_nref[sp] = nr;
+        int cnc[20] = {0};
+        cnc[0] = 1;
+        auto icn = [](double x) { long v = std::lround(x); return (int)std::min(19L, std::max(0L, v)); };
+        for (int r = 0; r < nr; r++) cnc[icn(REFCN[z - 1][r])]++;
+        for (int r = 0; r < nr; r++) {
+            int c = cnc[icn(REFCN[z - 1][r])];
+            sp_ngw[sp * 7 + r] = c * (c + 1) / 2;
+            sp_refcn[sp * 7 + r] = REFCOVCN[z - 1][r];
+            sp_refq[sp * 7 + r] = REFQ_GFN2[z - 1][r];
+        }
+        sp_zeff[sp] = EFFECTIVE_NUCLEAR_CHARGE[z - 1];
+        sp_gi[sp] = CHEMICAL_HARDNESS[z - 1] * 2.0;
+        sp_rcov[sp] = rcov_codata(z);
+        sp_en[sp] = PAULING_EN[z - 1];
+        r4r2[sp] = std::sqrt(0.5 * (R4_OVER_R2[z - 1] * std::sqrt((double)z)));
+        for (int ir = 0; ir < nr; ir++) {
+            int s2 = REFSYS[z - 1][ir];
+            if (s2 == 0) continue;
+            double iz = EFFECTIVE_NUCLEAR_CHARGE[s2 - 1], gam = CHEMICAL_HARDNESS[s2 - 1] * 2.0;
+            double qmod = REFH_GFN2[z - 1][ir] + iz;
+            double zv = qmod < 0.0 ? std::exp(3.0) : std::exp(3.0 * (1.0 - std::exp(gam * (1.0 - iz / qmod))));
+            for (int k = 0; k < 23; k++) {
+                double a = SSCALE[s2 - 1] * SECAIW[s2 - 1][k] * zv;
+                double v = ASCALE[z - 1][ir] * (ALPHAIW[z - 1][ir][k] - HCOUNT[z - 1][ir] * a);
+                aiw[((size_t)sp * 7 + ir) * 23 + k] = v > 0.0 ? v : 0.0;
+            }
+        }
+    }
+    double tw[23];
+    tw[0] = 0.5 * (FREQ[1] - FREQ[0]);
+    for (int k = 1; k < 22; k++) tw[k] = 0.5 * ((FREQ[k] - FREQ[k - 1]) + (FREQ[k + 1] - FREQ[k]));
+    tw[22] = 0.5 * (FREQ[22] - FREQ[21]);
+    for (int a = 0; a < nsp; a++)
+        for (int b = 0; b <= a; b++)
+            for (int r = 0; r < sp_nref[a]; r++)
+                for (int s = 0; s < sp_nref[b]; s++) {
+                    double acc = 0.0;
+                    for (int k = 0; k < 23; k++) acc += aiw[((size_t)a * 7 + r) * 23 + k] * aiw[((size_t)b * 7 + s) * 23 + k] * tw[k];
+                    double c6 = 3.0 / PI_ * acc;
+                    c6ref[((size_t)(a * nsp + b)) * 49 + r * 7 + s] = c6;
+                    c6ref[((size_t)(b * nsp + a)) * 49 + s * 7 + r] = c6;
+                }
+    for (int a = 0; a < nsp; a++)
+        for (int b = 0; b < nsp; b++) {
+            double v = 3.0 * r4r2[a] * r4r2[b];
+            sp_rr[a * nsp + b] = v;
+            sp_r0[a * nsp + b] = 0.52 * std::sqrt(v) + 5.0;
+        }
+    // ---- team plan: molecules from 1024 AOs on run on the whole grid, the rest one per CTA
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    int per = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, axg::k_team, axg::TEAM_THREADS, 0));
+    if (per <= 0) throw Fail(AXTB_ERR_DEVICE, "team kernel does not fit on a multiprocessor");
+    grid = nsm * std::min(per, 2);
+    vector<int> big, small_off(grid + 1, 0), small_list;
+    {
+        vector<std::pair<double, int>> smalls;
+        for (int m = 0; m < nmol; m++) {
+            if (m_nao[m] >= 1024) big.push_back(m);
+            else smalls.push_back({std::pow((double)m_nao[m] + 32.0, 3.0), m});
+        }
+        std::sort(smalls.begin(), smalls.end(), [](auto& x, auto& y) { return x.first > y.first; });
+        vector<vector<int>> lists(grid);
+        std::priority_queue<std::pair<double, int>, vector<std::pair<double, int>>, std::greater<>> pq;
+        for (int g = 0; g < grid; g++) pq.push({0.0, g});
+        for (auto& s : smalls) {
+            auto top = pq.top();
+            pq.pop();
+            lists[top.second].push_back(s.second);
+            pq.push({top.first + s.first, top.second});
+        }
+        for (int g = 0; g < grid; g++) {
+            small_off[g + 1] = small_off[g] + (int)lists[g].size();
+            for (int m : lists[g]) small_list.push_back(m);
+        }
+    }
+    // ---- device allocation (one arena)
+    size_t bytes = 0;
+    auto addI = [&](size_t n) { bytes += padded<int>(n); };
+    auto addD = [&](size_t n) { bytes += padded<double>(n); };
+    auto addL = [&](size_t n) { bytes += padded<long long>(n); };
+    addI(nmol * 7);
+    addL(nmol * 10);
+    addD(nmol * 3);
+    addI(natT * 6);
+    addD(natT * 15);
+    addI(nshT * 7);
+    addD((size_t)nshT * 12 + (size_t)nshT * 9);
+    addI(naoT * 2);
+    addI(nsp + nsp * 7);
+    addD(nsp * 7 * 2 + nsp * 4 + (size_t)nsp * nsp * 49 + (size_t)nsp * nsp * 2);
+    addI(big.size() + 1 + small_off.size() + small_list.size() + 1);
+    // state
+    addD(natT * 3 + natT * 6 + nshT * 2);
+    addD((size_t)nnT * 22);
+    bytes += padded<unsigned char>((size_t)nnT);
+    addD((size_t)naoT * 5);
+    addI(nmol * 7);
+    addD((size_t)nshT * 3 + (size_t)natT * 2 + (size_t)natT * 6 + (size_t)natT * 12 + (size_t)nshT + natT * 10);
+    addD((size_t)natT * 14);
+    addD((size_t)naoT * 11);
+    addD((size_t)nvecT * 4 + (size_t)nhist * 2 + (size_t)nmol * hist_cap * hist_cap * 2 + (size_t)nmol * hist_cap);
+    addD((size_t)nmol * 14);
+    addD((size_t)natT * 5 + (size_t)std::max(npairT, 1LL) * 5 + natT + natT * 5);
+    addD((size_t)grid * 8 + 64);
+    addD((size_t)nsqT * 3 + natT * 2);
+    addD((size_t)nwk);
+    addL(nmol * 5);
+    addD((size_t)nsqT * 2);
+    bytes += 1 << 20;
+    CK(cudaMalloc(&dmem, bytes));
+    Arena ar{(char*)dmem, bytes, 0};
+    auto upI = [&](const vector<int>& v) {
+        int* p = ar.take<int>(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        return (const int*)p;
+    };
+    auto upD = [&](const vector<double>& v) {
+        double* p = ar.take<double>(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        return (const double*)p;
+    };
+    auto upL = [&](const vector<long long>& v) {
+        long long* p = ar.take<long long>(std::max<size_t>(v.size(), 1));
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+        return p;
+    };
+    axg::Batch& b = B;
+    b.nmol = nmol;
+    b.natT = natT;
+    b.nshT = nshT;
+    b.naoT = naoT;
+    b.nnT = nnT;
+    b.npairT = npairT;
+    b.nvecT = nvecT;
+    b.nsp = nsp;
+    b.hist_cap = hist_cap;
+    b.m_nat = upI(m_nat);
+    b.m_nsh = upI(m_nsh);
+    b.m_nao = upI(m_nao);
+    b.m_at0 = upI(m_at0);
+    b.m_sh0 = upI(m_sh0);
+    b.m_ao0 = upI(m_ao0);
+    b.m_dim = upI(m_dim);
+    b.m_mat0 = upL(m_mat0);
+    b.m_vec0 = upL(m_vec0);
+    b.m_pair0 = upL(m_pair0);
+    d_pair0 = const_cast<long long*>(b.m_pair0);
+    b.m_hist0 = upL(m_hist0);
+    d_pd0 = upL(m_pd0);
+    d_tile0 = upL(m_tile0);
+    d_sq0 = upL(m_sq0);
+    b.m_nalpha = upD(m_na);
+    b.m_nbeta = upD(m_nb);
+    b.m_charge = upD(m_ch);
+    b.a_Z = upI(a_Z);
+    b.a_mol = upI(a_mol);
+    b.a_sh0 = upI(a_sh0);
+    b.a_nsh = upI(a_nsh);
+    b.a_ao0 = upI(a_ao0);
+    b.a_sp = upI(a_sp);
+    b.a_rcov = upD(a_rcov);
+    b.a_rad = upD(a_rad);
+    b.a_amin = upD(a_amin);
+    b.a_rcov_eeq = upD(a_rcov_eeq);
+    b.a_en = upD(a_en);
+    b.a_aes_rad = upD(a_aes_rad);
+    b.a_aes_vcn = upD(a_aes_vcn);
+    b.a_dk = upD(a_dk);
+    b.a_qk = upD(a_qk);
+    b.a_rep_alpha = upD(a_ra);
+    b.a_rep_zeff = upD(a_rz);
+    b.a_eeq_chi = upD(a_chi);
+    b.a_eeq_eta = upD(a_eta);
+    b.a_eeq_kcn = upD(a_kcn);
+    b.a_eeq_rad = upD(a_erad);
+    b.s_l = upI(s_l);
+    b.s_np = upI(s_np);
+    b.s_at = upI(s_at);
+    b.s_ao0 = upI(s_ao0);
+    b.s_ish = upI(s_ish);
+    b.s_mol = upI(s_mol);
+    b.s_Z = upI(s_Z);
+    b.s_alpha = upD(s_alpha);
+    b.s_coeff = upD(s_coeff);
+    b.s_amin = upD(s_amin);
+    b.s_se0 = upD(s_se0);
+    b.s_kcn = upD(s_kcn);
+    b.s_shpoly = upD(s_shpoly);
+    b.s_refocc = upD(s_refocc);
+    b.s_hard = upD(s_hard);
+    b.s_gam3 = upD(s_gam3);
+    b.s_slater = upD(s_slater);
+    b.o_sh = upI(o_sh);
+    b.o_at = upI(o_at);
+    b.sp_nref = upI(sp_nref);
+    b.sp_ngw = upI(sp_ngw);
+    b.sp_refcn = upD(sp_refcn);
+    b.sp_refq = upD(sp_refq);
+    b.sp_zeff = upD(sp_zeff);
+    b.sp_gi = upD(sp_gi);
+    b.sp_rcov = upD(sp_rcov);
+    b.sp_en = upD(sp_en);
+    b.sp_c6ref = upD(c6ref);
+    b.sp_rr = upD(sp_rr);
+    b.sp_r0 = upD(sp_r0);
+    b.intcut = std::max(25.0 - 10.0 * std::log10(o.acc), 20.0);  // crates/axtb/src/basis.rs:135-137
+    b.kt = o.etemp * KB_HARTREE;
+    b.damping = o.damping;
+    b.econv = 1e-6 * o.acc;
+    b.pconv = 2e-5 * o.acc;
+    b.max_iter = o.max_iter;
+    // state
+    axg::State& s = S;
+    s.xyz = ar.take<double>(natT * 3);
+    s.cn = ar.take<double>(natT);
+    s.cn_d4 = ar.take<double>(natT);
+    s.cn_eeq = ar.take<double>(natT);
+    s.mrad = ar.take<double>(natT);
+    s.dmrdcn = ar.take<double>(natT);
+    s.se = ar.take<double>(nshT);
+    s.dsedcn = ar.take<double>(nshT);
+    s.S = ar.take<double>(nnT);
+    s.H0 = ar.take<double>(nnT);
+    s.D = ar.take<double>(nnT * 3);
+    s.Q = ar.take<double>(nnT * 6);
+    s.Linv = ar.take<double>(nnT);
+    s.F = ar.take<double>(nnT);
+    s.Fp = ar.take<double>(nnT);
+    s.Z = ar.take<double>(nnT);
+    s.C = ar.take<double>(nnT);
+    s.P = ar.take<double>(nnT);
+    s.W = ar.take<double>(nnT);
+    s.scr1 = ar.take<double>(nnT);
+    s.scr2 = ar.take<double>(nnT);
+    s.scr3 = ar.take<double>(nnT);
+    s.piv = ar.take<unsigned char>(nnT);
+    s.emo = ar.take<double>(naoT);
+    s.focc = ar.take<double>(naoT);
+    s.dtri = ar.take<double>(naoT);
+    s.etri = ar.take<double>(naoT);
+    s.tau = ar.take<double>(naoT);
+    s.kocc = ar.take<int>(nmol);
+    s.status = ar.take<int>(nmol);
+    s.conv = ar.take<int>(nmol);
+    s.active = ar.take<int>(nmol);
+    s.niter = ar.take<int>(nmol);
+    s.iter = ar.take<int>(nmol);
+    s.qsh_in = ar.take<double>(nshT);
+    s.qsh_out = ar.take<double>(nshT);
+    s.vsh = ar.take<double>(nshT);
+    s.qat_in = ar.take<double>(natT);
+    s.qat_out = ar.take<double>(natT);
+    s.dp_in = ar.take<double>(natT * 3);
+    s.dp_out = ar.take<double>(natT * 3);
+    s.qp_in = ar.take<double>(natT * 6);
+    s.qp_out = ar.take<double>(natT * 6);
+    s.vat = ar.take<double>(natT);
+    s.vdp = ar.take<double>(natT * 3);
+    s.vqp = ar.take<double>(natT * 6);
+    s.gw = ar.take<double>(natT * 7);
+    s.dgw = ar.take<double>(natT * 7);
+    s.ao_part = ar.take<double>((size_t)naoT * 11);
+    s.q_in = ar.take<double>(nvecT);
+    s.dq = ar.take<double>(nvecT);
+    s.qlast = ar.take<double>(nvecT);
+    s.dqlast = ar.take<double>(nvecT);
+    s.df = ar.take<double>(nhist);
+    s.u = ar.take<double>(nhist);
+    s.amat = ar.take<double>((size_t)nmol * hist_cap * hist_cap * 2);
+    s.omega = ar.take<double>((size_t)nmol * hist_cap);
+    s.energy = ar.take<double>(nmol);
+    s.elast = ar.take<double>(nmol);
+    s.de = ar.take<double>(nmol);
+    s.res = ar.take<double>(nmol);
+    s.ts = ar.take<double>(nmol);
+    s.e_fixed = ar.take<double>(nmol);
+    s.terms = ar.take<double>((size_t)nmol * 8);
+    s.grad = ar.take<double>(natT * 3);
+    s.dedcn = ar.take<double>(natT);
+    s.dedcn_d4 = ar.take<double>(natT);
+    s.pair_buf = ar.take<double>((size_t)std::max(npairT, 1LL) * 5);
+    s.e_atom = ar.take<double>(natT);
+    s.e_terms = ar.take<double>(natT * 5);
+    s.red = ar.take<double>((size_t)grid * 8 + 64);
+    s.eeq_A = ar.take<double>((size_t)nsqT * 3);
+    // team plan
+    P.big = upI(big);
+    P.nbig = (int)big.size();
+    P.small_off = upI(small_off);
+    P.small_list = upI(small_list);
+    P.m_wk0 = upL(m_wk0);
+    P.wk = ar.take<double>(nwk);
+    P.m_sq0 = d_sq0;
+    P.eeq_rhs = ar.take<double>(natT);
+    P.eeq_q = ar.take<double>(natT);
+    P.eeq_plane = nsqT;
+    P.max_chunks = MAXCH;
+    d_wt = ar.take<double>(std::max(nsqT, 1LL));
+    d_tt = ar.take<double>(std::max(nsqT, 1LL));
+    d_eatm = ar.take<double>(nmol);
+    e_rep.assign(nmol, 0.0);
+    e_atm.assign(nmol, 0.0);
+    CK(cudaStreamSynchronize(st));
+}
+
+// ------------------------------------------------------------------ small kernels of the driver
+namespace axg {
+
+// per-molecule sum of an atom array (one CTA per molecule)
+__global__ void k_mol_sum(Batch B, const double* src, double* dst) {
+    int m = blockIdx.x;
+    if (m >= B.nmol) return;
+    double s = 0.0;
+    for (int a = threadIdx.x; a < B.m_nat[m]; a += blockDim.x) s += src[B.m_at0[m] + a];
+    s = cta_sum(s);
+    if (threadIdx.x == 0) dst[m] = s;
+}
+
+// start moments: EEQ charges split over the shells by reference occupation
+// (crates/axtb/src/xtb.rs:522-549), zero multipoles, packed SCC vector
+__global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq) {
+    int m = blockIdx.x;
+    if (m >= B.nmol) return;
+    int a0 = B.m_at0[m], nat = B.m_nat[m];
+    for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
+        double tot = 0.0;
+        for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) tot += B.s_refocc[s];
+        double qa = 0.0;
+        for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
+            double q = (use_eeq && tot > 0.0) ? qeeq[a] * B.s_refocc[s] / tot : 0.0;
+            S.qsh_in[s] = q;
+            qa += q;
+        }
+        S.qat_in[a] = qa;
+        for (int k = 0; k < 3; k++) S.dp_in[3 * a + k] = 0.0;
+        for (int k = 0; k < 6; k++) S.qp_in[6 * a + k] = 0.0;
+    }
+    __syncthreads();
+    pack_moment(B, m, S.qsh_in, S.dp_in, S.qp_in, S.q_in + B.m_vec0[m], threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) {
+        S.elast[m] = 0.0;
+        S.iter[m] = 0;
+        S.niter[m] = 0;
+        S.conv[m] = 0;
+        S.active[m] = S.status[m] == 0 ? 1 : 0;
+    }
+}
+
+// start of a warm SCF: the previous converged output moments of every molecule
+__global__ void k_start_warm(Batch B, State S) {
+    int m = blockIdx.x;
+    if (m >= B.nmol) return;
+    int a0 = B.m_at0[m], nat = B.m_nat[m], s0 = B.m_sh0[m], nsh = B.m_nsh[m];
+    for (int s = s0 + threadIdx.x; s < s0 + nsh; s += blockDim.x) S.qsh_in[s] = S.qsh_out[s];
+    for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
+        S.qat_in[a] = S.qat_out[a];
+        for (int k = 0; k < 3; k++) S.dp_in[3 * a + k] = S.dp_out[3 * a + k];
+        for (int k = 0; k < 6; k++) S.qp_in[6 * a + k] = S.qp_out[6 * a + k];
+    }
+    __syncthreads();
+    pack_moment(B, m, S.qsh_in, S.dp_in, S.qp_in, S.q_in + B.m_vec0[m], threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) {
+        S.elast[m] = 0.0;
+        S.iter[m] = 0;
+        S.niter[m] = 0;
+        S.conv[m] = 0;
+        S.active[m] = S.status[m] == 0 ? 1 : 0;
+    }
+}
+
+}  // namespace axg
+
+namespace {
+
+inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+void AxtbBatch::upload_positions(const double* x, bool device_ptr) {
+    CK(cudaMemcpyAsync(S.xyz, x, sizeof(double) * 3 * natT, device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       st));
+}
+
+void AxtbBatch::run(bool want_grad, bool warm) {
+    using namespace axg;
+    launches = 0;
+    auto L = [&](void) { launches++; };
+    const int T = 256;
+    long long nn = nnT;
+    // reset per-run state
+    CK(cudaMemsetAsync(S.status, 0, sizeof(int) * nmol, st));
+    CK(cudaMemsetAsync(S.S, 0, sizeof(double) * nn * 11, st));  // S, H0, D(3), Q(6) contiguous
+    CK(cudaMemsetAsync(S.grad, 0, sizeof(double) * natT * 3, st));
+    CK(cudaMemsetAsync(S.dedcn, 0, sizeof(double) * natT, st));
+    CK(cudaMemsetAsync(S.dedcn_d4, 0, sizeof(double) * natT, st));
+    CK(cudaMemsetAsync(S.e_atom, 0, sizeof(double) * natT, st));
+    CK(cudaMemsetAsync(S.terms, 0, sizeof(double) * nmol * 8, st));
+    CK(cudaMemsetAsync(S.ts, 0, sizeof(double) * nmol, st));
+    // geometry
+    k_cn<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+    L();
+    k_selfenergy<<<blocks_for(std::max(natT, nshT), T), T, 0, st>>>(B, S);
+    L();
+    k_repulsion<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+    L();
+    double* e_tmp = S.energy;  // per-molecule scratch for the fixed energies
+    k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, S.e_fixed);
+    L();
+    CK(cudaMemsetAsync(S.e_atom, 0, sizeof(double) * natT, st));
+    // D4 three-body at q = 0 with dgw/dCN weights
+    CK(cudaMemsetAsync(P.eeq_q, 0, sizeof(double) * natT, st));
+    k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1);
+    L();
+    k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT);
+    L();
+    k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0);
+    L();
+    k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm);
+    L();
+    (void)e_tmp;
+    // integrals
+    k_integrals<<<blocks_for(npdT, 128), 128, 0, st>>>(B, S, d_pd0, npdT);
+    L();
+    // overlap factorisation and EEQ start
+    void* args[] = {&B, &S, &P, nullptr};
+    int ph = PH_OVERLAP;
+    args[3] = &ph;
+    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
+    L();
+    bool eeq = opt.guess == 0 && !warm;
+    if (warm) {
+        k_start_warm<<<nmol, T, 0, st>>>(B, S);
+        L();
+    } else if (eeq) {
+        k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT);
+        L();
+        ph = PH_EEQ;
+        CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
+        L();
+    }
+    if (!warm) {
+        k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0);
+        L();
+    }
+    // SCF
+    vector<int> act(nmol);
+    for (int it = 1; it <= opt.max_iter; it++) {
+        k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0);
+        L();
+        k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+        L();
+        k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles);
+        L();
+        ph = PH_EIGEN;
+        CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
+        L();
+        k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S);
+        L();
+        k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S);
+        L();
+        k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2);
+        L();
+        k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+        L();
+        k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap);
+        L();
+        CK(cudaMemcpyAsync(act.data(), S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
+    }
+    if (!want_grad) return;
+    ph = PH_WDENS;
+    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
+    L();
+    if (npairT > 0) {
+        k_h0_gradient<<<blocks_for(npairT, 128), 128, 0, st>>>(B, S, d_pair0, npairT, S.pair_buf);
+        L();
+    }
+    k_h0_gather<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_pair0, S.pair_buf);
+    L();
+    k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 1);
+    L();
+    k_grad_pairs<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+    L();
+    k_cn_chain<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
+    L();
+    CK(cudaGetLastError());
+}
+
+#include "../../include/axtb_gpu_debug.h"
+#include "capi.cuh"

@@ -1,0 +1,336 @@
+// C ABI (include/axtb_gpu.h, include/axtb_gpu_debug.h) over the batch engine.
+#pragma once
+
+// total energies of the batch on the device: fixed (repulsion + ATM) + electronic
+namespace axg {
+__global__ void k_total_energy(int nmol, const double* erep, const double* eatm, const double* eel, double* out) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < nmol) out[m] = erep[m] + eatm[m] + eel[m];
+}
+}  // namespace axg
+
+static int status_code(int bits, int conv) {
+    if (bits & (axg::ST_HISTORY)) return AXTB_ERR_SCF_NOT_CONVERGED;
+    if (bits != 0) return AXTB_ERR_NUMERICAL;
+    if (!conv) return AXTB_ERR_SCF_NOT_CONVERGED;
+    return AXTB_OK;
+}
+
+void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
+    vector<double> eel(nmol), erep(nmol), eatm(nmol), terms((size_t)nmol * 8), de(nmol), res(nmol);
+    vector<int> st_(nmol), conv(nmol), nit(nmol);
+    vector<double> grad((size_t)natT * 3), qat(natT), dp((size_t)natT * 3), qp((size_t)natT * 6), qsh(nshT);
+    CK(cudaMemcpyAsync(eel.data(), S.energy, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(erep.data(), S.e_fixed, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(eatm.data(), d_eatm, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(terms.data(), S.terms, sizeof(double) * nmol * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(de.data(), S.de, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(res.data(), S.res, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(st_.data(), S.status, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(conv.data(), S.conv, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nit.data(), S.niter, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(qat.data(), S.qat_out, sizeof(double) * natT, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(dp.data(), S.dp_out, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(qp.data(), S.qp_out, sizeof(double) * natT * 6, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(qsh.data(), S.qsh_out, sizeof(double) * nshT, cudaMemcpyDeviceToHost, st));
+    if (want_grad) CK(cudaMemcpyAsync(grad.data(), S.grad, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int m = 0; m < nmol; m++) {
+        AxtbResult& r = outs[m];
+        int a0 = m_at0[m], nat = mols[m].nat;
+        r.energy = erep[m] + eatm[m] + eel[m];
+        for (int k = 0; k < 8; k++) r.terms[k] = terms[(size_t)m * 8 + k];
+        r.terms[0] = erep[m];
+        r.terms[1] += eatm[m];
+        r.iterations = nit[m];
+        r.converged = conv[m];
+        r.energy_change = de[m];
+        r.residual = res[m];
+        r.status = status_code(st_[m], conv[m]);
+        if (status) status[m] = r.status;
+        if (want_grad && r.gradient)
+            std::memcpy(r.gradient, grad.data() + (size_t)a0 * 3, sizeof(double) * nat * 3);
+        if (r.charges) std::memcpy(r.charges, qat.data() + a0, sizeof(double) * nat);
+        if (r.dpat) std::memcpy(r.dpat, dp.data() + (size_t)a0 * 3, sizeof(double) * nat * 3);
+        if (r.qpat) std::memcpy(r.qpat, qp.data() + (size_t)a0 * 6, sizeof(double) * nat * 6);
+        if (r.qsh) std::memcpy(r.qsh, qsh.data() + m_sh0[m], sizeof(double) * mols[m].nsh);
+        if (r.dipole) {
+            for (int k = 0; k < 3; k++) {
+                double s = 0.0;
+                for (int i = 0; i < nat; i++) s += qat[a0 + i] * mols[m].xyz[3 * i + k] + dp[(size_t)(a0 + i) * 3 + k];
+                r.dipole[k] = s;
+            }
+        }
+    }
+}
+
+struct AxtbHandle {
+    HostMol mol;
+    Opt opt;
+    AxtbBatch* batch = nullptr;
+    bool have_guess = false;
+    std::string err;
+    ~AxtbHandle() { delete batch; }
+};
+
+static Opt to_opt(const AxtbOptions* o) {
+    Opt r;
+    if (o) {
+        r.acc = o->accuracy;
+        r.etemp = o->etemp;
+        r.max_iter = o->max_iter;
+        r.damping = o->damping;
+        r.guess = o->guess;
+        r.precision = o->precision;
+        r.device = o->device;
+    }
+    return r;
+}
+
+static HostMol to_mol(const AxtbMol& m) {
+    HostMol h;
+    if (m.nat <= 0 || !m.numbers || !m.positions) throw Fail(AXTB_ERR_INPUT, "molecule has no atoms");
+    h.nat = m.nat;
+    h.Z.assign(m.numbers, m.numbers + m.nat);
+    h.xyz.assign(m.positions, m.positions + 3 * (size_t)m.nat);
+    h.charge = m.charge;
+    h.uhf = m.uhf;
+    check_molecule(h);
+    return h;
+}
+
+template <class F>
+static int guarded(std::string* sink, F&& f) {
+    try {
+        f();
+        return AXTB_OK;
+    } catch (const Fail& e) {
+        g_last_error = e.what();
+        if (sink) *sink = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        if (sink) *sink = e.what();
+        return AXTB_ERR_DEVICE;
+    }
+}
+
+extern "C" {
+
+void axtb_gpu_default_options(AxtbOptions* o) {
+    if (!o) return;
+    o->accuracy = 1.0;
+    o->etemp = 300.0;
+    o->max_iter = 250;
+    o->damping = 0.4;
+    o->guess = 0;
+    o->precision = 0;
+    o->device = 0;
+}
+
+int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao) {
+    int s = 0, a = 0;
+    for (int i = 0; i < nat; i++) {
+        int z = numbers[i];
+        if (z < 1 || z > 86) return AXTB_ERR_UNSUPPORTED_ELEMENT;
+        for (int k = 0; k < gfn2tab::NSHELL[z - 1]; k++) {
+            s++;
+            a += 2 * gfn2tab::ANG_SHELL[z - 1][k] + 1;
+        }
+    }
+    if (nsh) *nsh = s;
+    if (nao) *nao = a;
+    return AXTB_OK;
+}
+
+int axtb_gpu_create(const int32_t* numbers, int32_t nat, double charge, int32_t uhf, const AxtbOptions* opts,
+                    AxtbHandle** out) {
+    if (!out) return AXTB_ERR_INPUT;
+    *out = nullptr;
+    AxtbHandle* h = new AxtbHandle();
+    int rc = guarded(nullptr, [&] {
+        h->opt = to_opt(opts);
+        check_options(h->opt);
+        if (nat <= 0 || !numbers) throw Fail(AXTB_ERR_INPUT, "molecule has no atoms");
+        h->mol.nat = nat;
+        h->mol.Z.assign(numbers, numbers + nat);
+        h->mol.xyz.assign(3 * (size_t)nat, 0.0);
+        for (int i = 0; i < nat; i++) h->mol.xyz[3 * i] = 10.0 * i;  // placeholder positions, replaced per call
+        h->mol.charge = charge;
+        h->mol.uhf = uhf;
+        check_molecule(h->mol);
+    });
+    if (rc != AXTB_OK) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return AXTB_OK;
+}
+
+int axtb_gpu_singlepoint(AxtbHandle* h, const double* positions, int32_t want_gradient, AxtbResult* out) {
+    if (!h || !positions || !out) return AXTB_ERR_INPUT;
+    return guarded(&h->err, [&] {
+        HostMol m = h->mol;
+        m.xyz.assign(positions, positions + 3 * (size_t)m.nat);
+        check_molecule(m);
+        if (!h->batch) {
+            h->batch = new AxtbBatch();
+            h->batch->build({m}, h->opt);
+        }
+        AxtbBatch& b = *h->batch;
+        b.mols[0].xyz = m.xyz;
+        b.upload_positions(m.xyz.data(), false);
+        int32_t st = 0;
+        // warm start from the previous geometry's moments, then once more from the guess
+        // (crates/axtb/src/calculator.rs:194-206)
+        bool warm = h->have_guess;
+        b.run(want_gradient != 0, warm);
+        b.extract(out, &st, want_gradient != 0);
+        if (st != AXTB_OK && warm) {
+            b.run(want_gradient != 0, false);
+            b.extract(out, &st, want_gradient != 0);
+        }
+        h->have_guess = st == AXTB_OK;
+        if (st != AXTB_OK) {
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "SCF failed: status %d after %d iterations (dE %.3e, residual %.3e)", st,
+                          out->iterations, out->energy_change, out->residual);
+            throw Fail(st, msg);
+        }
+    });
+}
+
+void axtb_gpu_destroy(AxtbHandle* h) { delete h; }
+
+int axtb_gpu_last_error(const AxtbHandle* h, char* buf, size_t len) {
+    const std::string& s = h ? h->err : g_last_error;
+    if (buf && len > 0) {
+        size_t n = std::min(len - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return (int)s.size();
+}
+
+int axtb_gpu_batch_create(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, AxtbBatch** out) {
+    if (!out || !mols || nmol <= 0) return AXTB_ERR_INPUT;
+    *out = nullptr;
+    AxtbBatch* b = new AxtbBatch();
+    int rc = guarded(nullptr, [&] {
+        Opt o = to_opt(opts);
+        check_options(o);
+        vector<HostMol> v;
+        v.reserve(nmol);
+        for (int i = 0; i < nmol; i++) {
+            try {
+                v.push_back(to_mol(mols[i]));
+            } catch (const Fail& f) {
+                throw Fail(f.code, "molecule " + std::to_string(i) + ": " + f.what());
+            }
+        }
+        b->build(v, o);
+    });
+    if (rc != AXTB_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return AXTB_OK;
+}
+
+int axtb_gpu_batch_run(AxtbBatch* b, const double* positions, int32_t want_gradient, AxtbResult* outs, int32_t* status) {
+    if (!b || !outs) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        if (positions) {
+            size_t off = 0;
+            for (auto& m : b->mols) {
+                m.xyz.assign(positions + off, positions + off + 3 * (size_t)m.nat);
+                off += 3 * (size_t)m.nat;
+            }
+            b->upload_positions(positions, false);
+        } else {
+            vector<double> all;
+            for (auto& m : b->mols) all.insert(all.end(), m.xyz.begin(), m.xyz.end());
+            b->upload_positions(all.data(), false);
+        }
+        b->run(want_gradient != 0);
+        b->extract(outs, status, want_gradient != 0);
+    });
+}
+
+int axtb_gpu_batch_run_device(AxtbBatch* b, const double* d_positions, int32_t want_gradient, double* d_energy,
+                              double* d_gradient, int32_t* status) {
+    if (!b || !d_positions) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        b->upload_positions(d_positions, true);
+        b->run(want_gradient != 0);
+        if (d_energy) {
+            axg::k_total_energy<<<(b->nmol + 255) / 256, 256, 0, b->st>>>(b->nmol, b->S.e_fixed, b->d_eatm, b->S.energy,
+                                                                           d_energy);
+            b->launches++;
+        }
+        if (want_gradient && d_gradient)
+            CK(cudaMemcpyAsync(d_gradient, b->S.grad, sizeof(double) * 3 * b->natT, cudaMemcpyDeviceToDevice, b->st));
+        if (status) {
+            vector<int> st_(b->nmol), conv(b->nmol);
+            CK(cudaMemcpyAsync(st_.data(), b->S.status, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost, b->st));
+            CK(cudaMemcpyAsync(conv.data(), b->S.conv, sizeof(int) * b->nmol, cudaMemcpyDeviceToHost, b->st));
+            CK(cudaStreamSynchronize(b->st));
+            for (int m = 0; m < b->nmol; m++) status[m] = status_code(st_[m], conv[m]);
+        }
+    });
+}
+
+void* axtb_gpu_batch_stream(AxtbBatch* b) { return b ? (void*)b->st : nullptr; }
+
+int64_t axtb_gpu_batch_launches(const AxtbBatch* b) { return b ? b->launches : 0; }
+
+void axtb_gpu_batch_destroy(AxtbBatch* b) { delete b; }
+
+int axtb_gpu_batch(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, int32_t want_gradient, AxtbResult* outs,
+                   int32_t* status) {
+    AxtbBatch* b = nullptr;
+    int rc = axtb_gpu_batch_create(mols, nmol, opts, &b);
+    if (rc != AXTB_OK) return rc;
+    rc = axtb_gpu_batch_run(b, nullptr, want_gradient, outs, status);
+    axtb_gpu_batch_destroy(b);
+    return rc;
+}
+
+// ---- introspection (include/axtb_gpu_debug.h)
+int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out) {
+    if (!b || !out || mol < 0 || mol >= b->nmol) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        int nat = b->mols[mol].nat, n = b->mols[mol].nao;
+        long long a0 = b->m_at0[mol], o0 = b->m_ao0[mol], mat = b->m_mat0[mol], nn = b->nnT;
+        auto cp = [&](const double* src, size_t cnt) {
+            CK(cudaMemcpyAsync(out, src, sizeof(double) * cnt, cudaMemcpyDeviceToHost, b->st));
+        };
+        size_t n2 = (size_t)n * n;
+        switch (what) {
+            case AXTB_DBG_CN: cp(b->S.cn + a0, nat); break;
+            case AXTB_DBG_OVERLAP: cp(b->S.S + mat, n2); break;
+            case AXTB_DBG_H0: cp(b->S.H0 + mat, n2); break;
+            case AXTB_DBG_DIPOLE:
+                for (int k = 0; k < 3; k++)
+                    CK(cudaMemcpyAsync(out + k * n2, b->S.D + k * nn + mat, sizeof(double) * n2, cudaMemcpyDeviceToHost, b->st));
+                break;
+            case AXTB_DBG_QUADRUPOLE:
+                for (int k = 0; k < 6; k++)
+                    CK(cudaMemcpyAsync(out + k * n2, b->S.Q + k * nn + mat, sizeof(double) * n2, cudaMemcpyDeviceToHost, b->st));
+                break;
+            case AXTB_DBG_DENSITY: cp(b->S.P + mat, n2); break;
+            case AXTB_DBG_FOCK: cp(b->S.F + mat, n2); break;
+            case AXTB_DBG_EMO: cp(b->S.emo + o0, n); break;
+            case AXTB_DBG_FOCC: cp(b->S.focc + o0, n); break;
+            case AXTB_DBG_WDENSITY: cp(b->S.W + mat, n2); break;
+            case AXTB_DBG_EEQ: cp(b->P.eeq_q + a0, nat); break;
+            case AXTB_DBG_LINV: cp(b->S.Linv + mat, n2); break;
+            default: throw Fail(AXTB_ERR_INPUT, "unknown debug quantity");
+        }
+        CK(cudaStreamSynchronize(b->st));
+    });
+}
+
+}  // extern "C"

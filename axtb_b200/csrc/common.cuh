@@ -1,0 +1,128 @@
+// Device-side layout of a batch of molecules and small helpers shared by the kernels.
+//
+// Every quantity of every molecule lives in one flat array per kind, indexed globally:
+// atoms, shells and AOs of molecule m start at m_at0[m], m_sh0[m], m_ao0[m]; its dense AO
+// matrices (column-major, leading dimension nao_m) start at m_mat0[m] in each matrix plane;
+// its SCC vector (nsh + 9 nat entries) at m_vec0[m]; its atom pairs (i > j, packed
+// i(i-1)/2 + j) at m_pair0[m]. Kernels take global work indices and find their molecule
+// through these offsets, so one launch serves one molecule or thousands.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace axg {
+
+constexpr int MAXPRIM = 6;
+constexpr int MAXREF = 7;
+constexpr int NFREQ = 23;
+
+// Status bits of one molecule (per-molecule word on the device)
+enum : int {
+    ST_NOT_PD = 1,         // overlap (or EEQ) matrix not positive definite
+    ST_NONFINITE = 2,      // non-finite Fock matrix or energy
+    ST_FERMI = 4,          // electrons not placed by the Fermi search
+    ST_MIXER = 8,          // Broyden system singular
+    ST_INVIT = 16,         // inverse iteration produced a non-finite vector
+    ST_HISTORY = 32,       // Broyden history capacity exhausted
+    ST_TIMEOUT = 64,       // a bounded device wait gave up
+};
+
+struct Batch {
+    int nmol, natT, nshT, naoT;
+    long long nnT;      // sum of nao^2
+    long long npairT;   // sum of nat(nat-1)/2
+    long long nvecT;    // sum of SCC vector lengths
+    int nsp;            // distinct elements in the batch (D4 tables)
+    int hist_cap;       // Broyden history slots per molecule
+    // molecules
+    const int *m_nat, *m_nsh, *m_nao, *m_at0, *m_sh0, *m_ao0, *m_dim;
+    const long long *m_mat0, *m_vec0, *m_pair0, *m_hist0;
+    const double *m_nalpha, *m_nbeta, *m_charge;
+    // atoms
+    const int *a_Z, *a_mol, *a_sh0, *a_nsh, *a_ao0, *a_sp;
+    const double *a_rcov;      // GFN2 CN covalent radius (bohr)
+    const double *a_rad;       // H0 shell-polynomial atomic radius (bohr)
+    const double *a_amin;      // smallest primitive exponent of the atom
+    const double *a_rcov_eeq;  // EEQ-guess CN covalent radius (bohr)
+    const double *a_en;        // Pauling EN
+    const double *a_aes_rad, *a_aes_vcn, *a_dk, *a_qk;  // AES parameters
+    const double *a_rep_alpha, *a_rep_zeff;
+    const double *a_eeq_chi, *a_eeq_eta, *a_eeq_kcn, *a_eeq_rad;
+    // shells
+    const int *s_l, *s_np, *s_at, *s_ao0, *s_ish, *s_mol;
+    const double *s_alpha, *s_coeff;  // [shell][MAXPRIM]
+    const double *s_amin, *s_se0, *s_kcn, *s_shpoly, *s_refocc, *s_hard, *s_gam3, *s_slater;
+    const int *s_Z;
+    // AOs
+    const int *o_sh, *o_at;
+    // D4 species tables (batch species = distinct elements)
+    const int *sp_nref, *sp_ngw;      // nref[nsp], ngw[nsp][MAXREF]
+    const double *sp_refcn, *sp_refq, *sp_zeff, *sp_gi, *sp_rcov, *sp_en;  // per species (x MAXREF)
+    const double *sp_c6ref;           // [nsp*nsp][MAXREF][MAXREF]
+    const double *sp_rr, *sp_r0;      // [nsp*nsp]
+    double intcut;                    // primitive screening threshold
+    double kt;                        // electronic kT (Eh)
+    double damping;
+    double econv, pconv;
+    int max_iter;
+};
+
+// per-geometry and per-iteration device state
+struct State {
+    double* xyz;          // natT*3
+    // geometry intermediates
+    double *cn, *se, *dsedcn, *mrad, *dmrdcn, *cn_d4, *cn_eeq;
+    // AO matrices: planes of nnT doubles
+    double *S, *H0, *D, *Q;  // D: 3 planes, Q: 6 planes
+    double *Linv;
+    double *F, *Fp, *Z, *C, *P, *W;
+    double *scr1, *scr2, *scr3;  // nnT each: inverse-iteration / back-transform scratch
+    unsigned char* piv;          // nnT
+    double *emo, *focc;          // naoT
+    double *dtri, *etri, *tau;   // naoT: tridiagonal and Householder factors
+    int* kocc;                   // nmol
+    // SCC moments (input = mixed, output = Mulliken)
+    double *qsh_in, *qat_in, *dp_in, *qp_in;
+    double *qsh_out, *qat_out, *dp_out, *qp_out;
+    double *vsh, *vat, *vdp, *vqp;  // potentials of the last Fock build
+    double *gw, *dgw;               // D4 weights and their charge (or CN) derivatives [natT][MAXREF]
+    double *ao_part;                // naoT * 11: per-AO column dots (S, D3, Q6, H0)
+    // mixer
+    double *q_in, *dq, *qlast, *dqlast, *df, *u, *amat, *omega;  // vecs; df/u: hist x vec
+    int* iter;                      // nmol: mixer iteration counter
+    // per molecule scalars
+    double *energy, *elast, *de, *res, *ts, *e_fixed;  // nmol
+    double* terms;     // nmol*8
+    int* status;       // nmol
+    int* conv;         // nmol: 1 converged, 0 running
+    int* active;       // nmol: 1 while the SCF runs
+    int* niter;        // nmol: SCF iterations done
+    double *grad, *dedcn, *dedcn_d4;  // natT*3, natT, natT
+    double* pair_buf;  // npairT*8: per atom-pair gradient partials
+    double* e_atom;    // natT
+    double* e_terms;   // natT*5: ES2, ES3, AES, D4 two-body, band per atom
+    // cooperative scratch
+    double* red;       // reduction partials (grid-size * 8)
+    double* eeq_A;     // EEQ system matrices (sum (nat)^2)
+    long long* m_eeq0;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double sq(double x) { return x * x; }
+
+// molecule owning global work index g, given ascending per-molecule start offsets
+__device__ __forceinline__ int find_mol(const long long* off, int nmol, long long g) {
+    int lo = 0, hi = nmol - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+}  // namespace axg

@@ -1,0 +1,659 @@
+// Kernels of one SCF iteration over a batch (inactive molecules skip their work):
+// potentials of the input moments (ES2, ES3, AES2, self-consistent D4), the Fock matrix,
+// Mulliken moments of the new density with the band energy, the energy of the output moments,
+// and modified Broyden mixing with the convergence test. Then the pair terms of the gradient.
+#pragma once
+#include "common.cuh"
+#include "k_geometry.cuh"
+#include "k_integrals.cuh"
+
+namespace axg {
+
+constexpr double SQRT2 = 1.4142135623730951;
+__constant__ double QSCALE[6] = {1.0, 2.0, 1.0, 2.0, 2.0, 1.0};
+__constant__ int QOFF[6] = {0, 1, 0, 1, 1, 0};
+
+__device__ __forceinline__ bool mol_active(const State& S, int m) { return S.active[m] != 0; }
+
+// ES2 kernel element (crates/axtb/src/coulomb.rs:61-119, g = 2); same atom: eta
+__device__ __forceinline__ double gamma_el(const Batch& B, const double* x, int sa, int sb) {
+    int a = B.s_at[sa], b = B.s_at[sb];
+    double eta = 0.5 * (B.s_hard[sa] + B.s_hard[sb]);
+    if (a == b) return eta;
+    double v[3];
+    dvec(x, a, b, v);
+    double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    return 1.0 / sqrt(r2 + 1.0 / (eta * eta));
+}
+
+// AES pair factors g3 = f3/r^3, g5 = f5/r^5 (crates/axtb/src/coulomb.rs:382-394)
+__device__ __forceinline__ void aes_g35(const State& S, int a, int b, double r2, double& g3, double& g5) {
+    double r1 = sqrt(r2), g1 = 1.0 / r1;
+    double gg3 = g1 * g1 * g1, gg5 = gg3 * g1 * g1;
+    double rr = 0.5 * (S.mrad[b] + S.mrad[a]) * g1;
+    double rr3 = rr * rr * rr;
+    g3 = gg3 * (1.0 / (1.0 + 6.0 * rr3));
+    g5 = gg5 * (1.0 / (1.0 + 6.0 * rr3 * rr));
+}
+
+// potentials of the input moments: warp per atom (shell potentials of the atom's shells, atom,
+// dipole and quadrupole potentials); crates/axtb/src/xtb.rs:316-340 with coulomb.rs:407-502,
+// 1006-1021, 1141-1143 and crates/d4/src/disp.rs:420-455
+__global__ void k_potentials(Batch B, State S) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    if (!mol_active(S, mv.m)) return;
+    const double* x = S.xyz;
+    int sh0 = B.m_sh0[mv.m], nsh = B.m_nsh[mv.m];
+    // ES2 + ES3 for the shells of atom a
+    for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
+        double v = 0.0;
+        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gamma_el(B, x, s, t) * S.qsh_in[t];
+        v = warp_sum(v);
+        if (lane == 0) S.vsh[s] = v + S.qsh_in[s] * S.qsh_in[s] * B.s_gam3[s];
+    }
+    // AES and D4 atom potentials
+    double va = 0.0, vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
+    int spa = B.a_sp[a];
+    for (int b = mv.i0 + lane; b < mv.i0 + mv.n; b += 32) {
+        if (b == a) continue;
+        double w[3];
+        dvec(x, a, b, w);
+        double r2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+        double g3, g5;
+        aes_g35(S, a, b, r2, g3, g5);
+        const double* mb = S.dp_in + 3 * b;
+        double qb = S.qat_in[b];
+        double mbw = mb[0] * w[0] + mb[1] * w[1] + mb[2] * w[2];
+        va += mbw * g3;
+        for (int k = 0; k < 3; k++) vd[k] += -w[k] * g3 * qb + g5 * (r2 * mb[k] - 3.0 * w[k] * mbw);
+        double tc[6] = {w[0] * w[0], w[0] * w[1], w[1] * w[1], w[0] * w[2], w[1] * w[2], w[2] * w[2]};
+        double thb = 0.0;
+        for (int k = 0; k < 6; k++) {
+            double t = QSCALE[k] * tc[k] * g5;
+            vq[k] += t * qb;
+            thb += t * S.qp_in[6 * b + k];
+        }
+        va += thb;
+        // D4: -dC6/dq_a * pair factor
+        double pe, pg;
+        if (d4_pair(B, spa, B.a_sp[b], r2, pe, pg)) {
+            double c6, da, db;
+            pair_c6(B, S, a, b, c6, da, db);
+            va -= da * pe;
+        }
+    }
+    va = warp_sum(va);
+    for (int k = 0; k < 3; k++) vd[k] = warp_sum(vd[k]);
+    for (int k = 0; k < 6; k++) vq[k] = warp_sum(vq[k]);
+    if (lane == 0) {
+        S.vat[a] = va;
+        for (int k = 0; k < 3; k++) S.vdp[3 * a + k] = vd[k] + 2.0 * B.a_dk[a] * S.dp_in[3 * a + k];
+        for (int k = 0; k < 6; k++) S.vqp[6 * a + k] = vq[k] + 2.0 * B.a_qk[a] * S.qp_in[6 * a + k] * QSCALE[k];
+    }
+}
+
+// Fock matrix F = H0 - (B + B^T)/2, B(mu,nu) = S v_ao(nu) + D.v_d(A_nu) + Q.v_q(A_nu)
+// (crates/axtb/src/scf/fock.rs:22-104). One 32x32 tile per CTA (32x8 threads), the transposed
+// half of each pair of elements staged through shared memory.
+__device__ __forceinline__ double bterm(const Batch& B, const State& S, long long e, int ao_col) {
+    int at = B.o_at[ao_col];
+    double v = S.vsh[B.o_sh[ao_col]] + S.vat[at];
+    long long nn = B.nnT;
+    double x = S.S[e] * v;
+    for (int k = 0; k < 3; k++) x += S.D[k * nn + e] * S.vdp[3 * at + k];
+    for (int k = 0; k < 6; k++) x += S.Q[k * nn + e] * S.vqp[6 * at + k];
+    return x;
+}
+
+__global__ void k_fock(Batch B, State S, const long long* m_tile0, long long ntiles) {
+    __shared__ double bt[32][33];
+    long long tile = blockIdx.x;
+    if (tile >= ntiles) return;
+    int m = find_mol(m_tile0, B.nmol, tile);
+    if (!mol_active(S, m)) return;
+    int n = B.m_nao[m], ao0 = B.m_ao0[m];
+    int nt = (n + 31) / 32;
+    long long lt = tile - m_tile0[m];
+    int ti = (int)(lt % nt), tj = (int)(lt / nt);
+    long long mat = B.m_mat0[m];
+    int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    // transposed tile: element (J + a, I + b) for a = tx, b = ty..
+    for (int b = ty; b < 32; b += 8) {
+        int row = tj * 32 + tx, col = ti * 32 + b;
+        double v = 0.0;
+        if (row < n && col < n) v = bterm(B, S, mat + row + (long long)col * n, ao0 + col);
+        bt[b][tx] = v;
+    }
+    __syncthreads();
+    for (int b = ty; b < 32; b += 8) {
+        int row = ti * 32 + tx, col = tj * 32 + b;
+        if (row >= n || col >= n) continue;
+        long long e = mat + row + (long long)col * n;
+        double f = S.H0[e] - 0.5 * (bterm(B, S, e, ao0 + col) + bt[tx][b]);
+        if (!isfinite(f)) atomicOr(&S.status[m], ST_NONFINITE);
+        S.F[e] = f;
+    }
+}
+
+// Mulliken column dots (crates/axtb/src/scf/mulliken.rs:19-59) and the band energy column
+// (crates/axtb/src/xtb.rs:1129-1135): warp per AO column; out[nu*11 + k]
+__global__ void k_mulliken(Batch B, State S) {
+    int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (g >= B.naoT) return;
+    int at = B.o_at[g], m = B.a_mol[at];
+    if (!mol_active(S, m)) return;
+    int n = B.m_nao[m], nu = g - B.m_ao0[m];
+    long long col = B.m_mat0[m] + (long long)nu * n, nn = B.nnT;
+    double r[11];
+    for (int k = 0; k < 11; k++) r[k] = 0.0;
+    for (int mu = lane; mu < n; mu += 32) {
+        long long e = col + mu;
+        double p = S.P[e];
+        r[0] += p * S.S[e];
+        for (int k = 0; k < 3; k++) r[1 + k] += p * S.D[k * nn + e];
+        for (int k = 0; k < 6; k++) r[4 + k] += p * S.Q[k * nn + e];
+        r[10] += p * S.H0[e];
+    }
+    for (int k = 0; k < 11; k++) r[k] = warp_sum(r[k]);
+    if (lane == 0)
+        for (int k = 0; k < 11; k++) S.ao_part[(long long)g * 11 + k] = r[k];
+}
+
+// output moments from the column dots: thread per atom (its shells and AOs in order)
+__global__ void k_moments(Batch B, State S) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= B.natT) return;
+    int m = B.a_mol[a];
+    if (!mol_active(S, m)) return;
+    double dp[3] = {0, 0, 0}, qp[6] = {0, 0, 0, 0, 0, 0}, qa = 0.0, band = 0.0;
+    for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
+        double q = B.s_refocc[s];
+        for (int o = B.s_ao0[s]; o < B.s_ao0[s] + 2 * B.s_l[s] + 1; o++) {
+            const double* r = S.ao_part + (long long)o * 11;
+            q -= r[0];
+            for (int k = 0; k < 3; k++) dp[k] -= r[1 + k];
+            for (int k = 0; k < 6; k++) qp[k] -= r[4 + k];
+            band += r[10];
+        }
+        S.qsh_out[s] = q;
+        qa += q;
+    }
+    S.qat_out[a] = qa;
+    for (int k = 0; k < 3; k++) S.dp_out[3 * a + k] = dp[k];
+    for (int k = 0; k < 6; k++) S.qp_out[6 * a + k] = qp[k];
+    S.e_atom[a] = band;  // band part of the atom's electronic energy; the rest is added next
+    S.e_terms[5 * a + 4] = band;
+}
+
+// electronic energy per atom of the output moments (crates/axtb/src/xtb.rs:1058-1146): ES2 and
+// ES3 of its shells, half of its AES pair energies plus its on-site AES, half of its D4
+// two-body pair energies (weights at the output charges), plus the band part from k_moments
+__global__ void k_energy(Batch B, State S) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    if (!mol_active(S, mv.m)) return;
+    const double* x = S.xyz;
+    int sh0 = B.m_sh0[mv.m], nsh = B.m_nsh[mv.m];
+    double e = 0.0, e2 = 0.0, e3 = 0.0, eaes = 0.0, ed = 0.0;
+    for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
+        double v = 0.0;
+        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gamma_el(B, x, s, t) * S.qsh_out[t];
+        v = warp_sum(v);
+        double q = S.qsh_out[s];
+        e2 += 0.5 * q * v;
+        e3 += q * q * q * B.s_gam3[s] / 3.0;
+    }
+    int spa = B.a_sp[a];
+    const double* di = S.dp_out + 3 * a;
+    const double* ti = S.qp_out + 6 * a;
+    double qi = S.qat_out[a];
+    for (int b = mv.i0 + lane; b < mv.i0 + mv.n; b += 32) {
+        if (b == a) continue;
+        double v[3];
+        dvec(x, a, b, v);
+        double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        double g3, g5;
+        aes_g35(S, a, b, r2, g3, g5);
+        const double* dj = S.dp_out + 3 * b;
+        const double* tj = S.qp_out + 6 * b;
+        double qj = S.qat_out[b];
+        double miv = di[0] * v[0] + di[1] * v[1] + di[2] * v[2];
+        double mjv = dj[0] * v[0] + dj[1] * v[1] + dj[2] * v[2];
+        double ep = (qi * mjv - qj * miv) * g3;
+        ep += g5 * (r2 * (di[0] * dj[0] + di[1] * dj[1] + di[2] * dj[2]) - 3.0 * miv * mjv);
+        double tc[6] = {v[0] * v[0], v[0] * v[1], v[1] * v[1], v[0] * v[2], v[1] * v[2], v[2] * v[2]};
+        for (int k = 0; k < 6; k++) ep += QSCALE[k] * tc[k] * g5 * (qj * ti[k] + qi * tj[k]);
+        eaes += 0.5 * ep;
+        double pe, pg;
+        if (d4_pair(B, spa, B.a_sp[b], r2, pe, pg)) {
+            double c6, da, db;
+            pair_c6(B, S, a, b, c6, da, db);
+            ed -= 0.5 * c6 * pe;
+        }
+    }
+    eaes = warp_sum(eaes);
+    ed = warp_sum(ed);
+    if (lane == 0) {
+        double qq = 0.0;
+        for (int k = 0; k < 6; k++) qq += QSCALE[k] * ti[k] * ti[k];
+        eaes += B.a_dk[a] * (di[0] * di[0] + di[1] * di[1] + di[2] * di[2]) + B.a_qk[a] * qq;
+        e = e2 + e3 + eaes + ed;
+        S.e_atom[a] += e;
+        // term pieces per atom (reduced per molecule in k_broyden)
+        S.e_terms[5 * a + 0] = e2;
+        S.e_terms[5 * a + 1] = e3;
+        S.e_terms[5 * a + 2] = eaes;
+        S.e_terms[5 * a + 3] = ed;
+    }
+}
+
+// ----------------------------------------------------------------------------- Broyden
+__device__ double cta_sum(double v) {
+    __shared__ double red[32];
+    __shared__ double out;
+    v = warp_sum(v);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += red[k];
+        out = s;
+    }
+    __syncthreads();
+    return out;
+}
+
+__device__ __forceinline__ void pack_moment(const Batch& B, int m, const double* qsh, const double* dp, const double* qp,
+                                            double* v, int tid, int nthr) {
+    int nsh = B.m_nsh[m], nat = B.m_nat[m], s0 = B.m_sh0[m], a0 = B.m_at0[m];
+    for (int i = tid; i < nsh + 9 * nat; i += nthr) {
+        double x;
+        if (i < nsh) x = qsh[s0 + i];
+        else if (i < nsh + 3 * nat) x = dp[3 * a0 + (i - nsh)];
+        else {
+            int r = i - nsh - 3 * nat, c = r % 6;
+            x = qp[6 * a0 + r] * (QOFF[c] ? SQRT2 : 1.0);
+        }
+        v[i] = x;
+    }
+}
+
+// energy assembly, residual, convergence test (crates/axtb/src/scf/convergence.rs:99-130) and
+// the next input by modified Broyden mixing (crates/axtb/src/scf/mixing.rs:251-338 with
+// crates/base/src/linalg/lu.rs:81-112); one CTA per molecule
+__global__ void k_broyden(Batch B, State S, int hist_cap) {
+    int m = blockIdx.x;
+    if (m >= B.nmol || !mol_active(S, m)) return;
+    int tid = threadIdx.x, nthr = blockDim.x;
+    int dim = B.m_dim[m], nat = B.m_nat[m], a0 = B.m_at0[m];
+    long long v0 = B.m_vec0[m];
+    double* q_in = S.q_in + v0;
+    double* dq = S.dq + v0;
+    double* qlast = S.qlast + v0;
+    double* dqlast = S.dqlast + v0;
+    long long h0 = B.m_hist0[m];
+    double* df = S.df + h0 * 1;  // hist_cap * dim
+    double* u = S.u + h0 * 1;
+    double* amat = S.amat + (long long)m * hist_cap * hist_cap;
+    double* omega = S.omega + (long long)m * hist_cap;
+    // energy and terms (sums in atom order per thread stripe, reduced deterministically)
+    double e = 0.0, t2 = 0.0, t3 = 0.0, ta = 0.0, td = 0.0, tb = 0.0;
+    for (int a = tid; a < nat; a += nthr) {
+        e += S.e_atom[a0 + a];
+        t2 += S.e_terms[5 * (a0 + a) + 0];
+        t3 += S.e_terms[5 * (a0 + a) + 1];
+        ta += S.e_terms[5 * (a0 + a) + 2];
+        td += S.e_terms[5 * (a0 + a) + 3];
+        tb += S.e_terms[5 * (a0 + a) + 4];
+    }
+    e = cta_sum(e) + S.ts[m];
+    t2 = cta_sum(t2);
+    t3 = cta_sum(t3);
+    ta = cta_sum(ta);
+    td = cta_sum(td);
+    tb = cta_sum(tb);
+    // residual dq = pack(out) - q_in
+    pack_moment(B, m, S.qsh_out, S.dp_out, S.qp_out, dq, tid, nthr);
+    __syncthreads();
+    double rr = 0.0;
+    for (int i = tid; i < dim; i += nthr) {
+        dq[i] -= q_in[i];
+        rr += dq[i] * dq[i];
+    }
+    rr = cta_sum(rr);
+    __shared__ int s_done, s_ok;
+    if (tid == 0) {
+        double res = sqrt(rr / dim);
+        double de = e - S.elast[m];
+        S.elast[m] = e;
+        S.energy[m] = e;
+        S.de[m] = de;
+        S.res[m] = res;
+        double* tm = S.terms + 8 * m;
+        tm[2] = e;
+        tm[3] = t2;
+        tm[4] = t3;
+        tm[5] = ta;
+        tm[1] = td;
+        tm[6] = S.ts[m];
+        tm[7] = tb;
+        int it = ++S.niter[m];
+        if (!isfinite(e)) S.status[m] |= ST_NONFINITE;
+        bool ok = fabs(de) < B.econv && res < B.pconv;
+        s_done = 0;
+        if (S.status[m] != 0) {
+            S.active[m] = 0;
+            s_done = 1;
+        } else if (ok) {
+            S.conv[m] = 1;
+            S.active[m] = 0;
+            s_done = 1;
+        } else if (it >= B.max_iter) {
+            S.active[m] = 0;
+            s_done = 1;
+        }
+    }
+    __syncthreads();
+    if (s_done) return;
+    // ---- Broyden step
+    int iter = ++S.iter[m];
+    double alpha = B.damping;
+    if (iter == 1) {
+        for (int i = tid; i < dim; i += nthr) {
+            dqlast[i] = dq[i];
+            qlast[i] = q_in[i];
+            q_in[i] += alpha * dq[i];
+        }
+    } else {
+        int itn = iter - 1;
+        int it1 = itn - 1;
+        if (it1 >= hist_cap) {
+            if (tid == 0) {
+                S.status[m] |= ST_HISTORY;
+                S.active[m] = 0;
+            }
+            return;
+        }
+        int nh = itn;  // memory = max_iter >= iterations: the whole history
+        double* dfi = df + (long long)it1 * dim;
+        double nr = 0.0;
+        for (int i = tid; i < dim; i += nthr) nr += dq[i] * dq[i];
+        nr = sqrt(cta_sum(nr));
+        const double OMEGA0 = 0.01, MINW = 1.0, MAXW = 100000.0, WFAC = 0.01;
+        double om = nr > WFAC / MAXW ? WFAC / nr : MAXW;
+        if (om < MINW) om = MINW;
+        if (tid == 0) omega[it1] = om;
+        double dn = 0.0;
+        for (int i = tid; i < dim; i += nthr) {
+            double v = dq[i] - dqlast[i];
+            dfi[i] = v;
+            dn += v * v;
+        }
+        dn = cta_sum(dn);
+        double inv = 1.0 / fmax(sqrt(dn), DBL_EPSILON);
+        for (int i = tid; i < dim; i += nthr) dfi[i] *= inv;
+        __syncthreads();
+        // a[it1][j] = df_it1 . df_j (j <= it1), c[j] = omega_j df_j . dq
+        __shared__ double cvec[128];
+        for (int j = 0; j < nh; j++) {
+            double* dfj = df + (long long)j * dim;
+            double s1 = 0.0, s2 = 0.0;
+            for (int i = tid; i < dim; i += nthr) {
+                s1 += dfi[i] * dfj[i];
+                s2 += dfj[i] * dq[i];
+            }
+            s1 = cta_sum(s1);
+            s2 = cta_sum(s2);
+            if (tid == 0) {
+                amat[it1 * hist_cap + j] = s1;
+                amat[j * hist_cap + it1] = s1;
+                cvec[j] = s2;  // times omega below
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            s_ok = 1;
+            // Gauss elimination with the last largest pivot on beta (kept in the tail of amat's slab)
+            double* bt = S.amat + (long long)B.nmol * hist_cap * hist_cap + (long long)m * hist_cap * hist_cap;
+            for (int i = 0; i < nh; i++) {
+                cvec[i] *= omega[i];
+                for (int j = 0; j < nh; j++) bt[i * hist_cap + j] = omega[i] * omega[j] * amat[i * hist_cap + j];
+                bt[i * hist_cap + i] += OMEGA0 * OMEGA0;
+            }
+            for (int col = 0; col < nh && s_ok; col++) {
+                int piv = col;
+                for (int i = col + 1; i < nh; i++)
+                    if (fabs(bt[i * hist_cap + col]) >= fabs(bt[piv * hist_cap + col])) piv = i;
+                if (bt[piv * hist_cap + col] == 0.0) {
+                    s_ok = 0;
+                    break;
+                }
+                if (piv != col) {
+                    for (int k = 0; k < nh; k++) {
+                        double tmp = bt[col * hist_cap + k];
+                        bt[col * hist_cap + k] = bt[piv * hist_cap + k];
+                        bt[piv * hist_cap + k] = tmp;
+                    }
+                    double tmp = cvec[col];
+                    cvec[col] = cvec[piv];
+                    cvec[piv] = tmp;
+                }
+                for (int row = col + 1; row < nh; row++) {
+                    double f = bt[row * hist_cap + col] / bt[col * hist_cap + col];
+                    if (f != 0.0) {
+                        for (int k = col; k < nh; k++) bt[row * hist_cap + k] -= f * bt[col * hist_cap + k];
+                        cvec[row] -= f * cvec[col];
+                    }
+                }
+            }
+            if (s_ok)
+                for (int col = nh - 1; col >= 0; col--) {
+                    double s = cvec[col];
+                    for (int k = col + 1; k < nh; k++) s -= bt[col * hist_cap + k] * cvec[k];
+                    cvec[col] = s / bt[col * hist_cap + col];
+                }
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) {
+                S.status[m] |= ST_MIXER;
+                S.active[m] = 0;
+            }
+            return;
+        }
+        double* ui = u + (long long)it1 * dim;
+        for (int i = tid; i < dim; i += nthr) {
+            ui[i] = alpha * dfi[i] + inv * (q_in[i] - qlast[i]);
+            dqlast[i] = dq[i];
+            qlast[i] = q_in[i];
+            double v = q_in[i] + alpha * dq[i];
+            for (int j = 0; j < nh; j++) v -= omega[j] * cvec[j] * u[(long long)j * dim + i];
+            q_in[i] = v;
+        }
+    }
+    __syncthreads();
+    // unpack the new input (and re-pack it, as the reference packs its unpacked state)
+    int nsh = B.m_nsh[m], s0 = B.m_sh0[m];
+    for (int i = tid; i < dim; i += nthr) {
+        double x = q_in[i];
+        if (i < nsh) S.qsh_in[s0 + i] = x;
+        else if (i < nsh + 3 * nat) S.dp_in[3 * a0 + (i - nsh)] = x;
+        else {
+            int r = i - nsh - 3 * nat, c = r % 6;
+            double y = x / (QOFF[c] ? SQRT2 : 1.0);
+            S.qp_in[6 * a0 + r] = y;
+            q_in[i] = y * (QOFF[c] ? SQRT2 : 1.0);
+        }
+    }
+    __syncthreads();
+    for (int a = tid; a < nat; a += nthr) {
+        double q = 0.0;
+        for (int s = B.a_sh0[a0 + a]; s < B.a_sh0[a0 + a] + B.a_nsh[a0 + a]; s++) q += S.qsh_in[s];
+        S.qat_in[a0 + a] = q;
+    }
+}
+
+// ----------------------------------------------------------------------------- gradient pairs
+// ES2 (crates/axtb/src/coulomb.rs:123-169), AES (896-1001) and D4 two-body at fixed charges
+// (crates/d4/src/disp.rs:460-484; weights and dgw/dCN at the output charges) per atom; warp per atom
+__global__ void k_grad_pairs(Batch B, State S) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    if (!S.conv[mv.m]) return;
+    const double* x = S.xyz;
+    double g[3] = {0, 0, 0}, dedr = 0.0, dcn4 = 0.0;
+    const double kdmp3 = 3.0, kdmp5 = 4.0;
+    int spa = B.a_sp[a];
+    for (int b = mv.i0 + lane; b < mv.i0 + mv.n; b += 32) {
+        if (b == a) continue;
+        double v[3];
+        dvec(x, a, b, v);  // R_a - R_b
+        double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        double r1 = sqrt(r2);
+        // ES2
+        double dg = 0.0;
+        for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++)
+            for (int t = B.a_sh0[b]; t < B.a_sh0[b] + B.a_nsh[b]; t++) {
+                double eta = 0.5 * (B.s_hard[s] + B.s_hard[t]);
+                double dt = 1.0 / (r2 + 1.0 / (eta * eta));
+                dt = -dt * sqrt(dt);
+                dg += dt * S.qsh_out[s] * S.qsh_out[t];
+            }
+        for (int k = 0; k < 3; k++) g[k] += dg * v[k];
+        // AES: the reference's pair (iat, jat) with vec = R_jat - R_iat; here (a, b) as (i, j)
+        {
+            double rr = 0.5 * (S.mrad[a] + S.mrad[b]);
+            double vec[3] = {-v[0], -v[1], -v[2]};
+            double g1 = 1.0 / r1, g3 = g1 * g1 * g1, g5 = g3 * g1 * g1, g7 = g5 * g1 * g1;
+            double rg = rr * g1, rg3 = rg * rg * rg, rg4 = rg3 * rg;
+            double fdmp3 = 1.0 / (1.0 + 6.0 * rg3);
+            double ddmp3 = -3.0 * g5 * fdmp3 - kdmp3 * fdmp3 * (fdmp3 - 1.0) * g5;
+            double fdmp5 = 1.0 / (1.0 + 6.0 * rg4);
+            double ddmp5 = -5.0 * fdmp5 - kdmp5 * (fdmp5 * fdmp5 - fdmp5);
+            double qi = S.qat_out[a], qj = S.qat_out[b];
+            const double* di = S.dp_out + 3 * a;
+            const double* dj = S.dp_out + 3 * b;
+            double dpiqj = (vec[0] * di[0] + vec[1] * di[1] + vec[2] * di[2]) * qj;
+            double qidpj = (vec[0] * dj[0] + vec[1] * dj[1] + vec[2] * dj[2]) * qi;
+            double fddr = 3.0 * (dpiqj - qidpj) * kdmp3 * fdmp3 * g3 * (fdmp3 / rr) * rg3;
+            double gg[3];
+            for (int k = 0; k < 3; k++) gg[k] = -ddmp3 * vec[k] * (dpiqj - qidpj) + fdmp3 * g3 * (qi * dj[k] - qj * di[k]);
+            double dpidpj = dj[0] * di[0] + dj[1] * di[1] + dj[2] * di[2];
+            double dpiv = di[0] * vec[0] + di[1] * vec[1] + di[2] * vec[2];
+            double dpjv = dj[0] * vec[0] + dj[1] * vec[1] + dj[2] * vec[2];
+            double edd = dpidpj * r2 - 3.0 * dpjv * dpiv;
+            fddr += 3.0 * edd * kdmp5 * fdmp5 * g5 * (fdmp5 / rr) * rg4;
+            for (int k = 0; k < 3; k++)
+                gg[k] += -2.0 * fdmp5 * g5 * dpidpj * vec[k] + 3.0 * fdmp5 * g5 * (dpiv * dj[k] + dpjv * di[k]) -
+                         edd * ddmp5 * g7 * vec[k];
+            const double* ti = S.qp_out + 6 * a;
+            const double* tj = S.qp_out + 6 * b;
+            double eq = 2.0 * (qj * ti[1] + tj[1] * qi) * vec[0] * vec[1] + 2.0 * (qj * ti[3] + tj[3] * qi) * vec[0] * vec[2] +
+                        2.0 * (qj * ti[4] + tj[4] * qi) * vec[1] * vec[2] + (qj * ti[0] + tj[0] * qi) * vec[0] * vec[0] +
+                        (qj * ti[2] + tj[2] * qi) * vec[1] * vec[1] + (qj * ti[5] + tj[5] * qi) * vec[2] * vec[2];
+            fddr += eq * 3.0 * kdmp5 * fdmp5 * g5 * fdmp5 / rr * rg4;
+            double tvj[3] = {vec[0] * tj[0] + vec[1] * tj[1] + vec[2] * tj[3], vec[0] * tj[1] + vec[1] * tj[2] + vec[2] * tj[4],
+                             vec[0] * tj[3] + vec[1] * tj[4] + vec[2] * tj[5]};
+            double tvi[3] = {vec[0] * ti[0] + vec[1] * ti[1] + vec[2] * ti[3], vec[0] * ti[1] + vec[1] * ti[2] + vec[2] * ti[4],
+                             vec[0] * ti[3] + vec[1] * ti[4] + vec[2] * ti[5]};
+            for (int k = 0; k < 3; k++)
+                gg[k] += -eq * ddmp5 * g7 * vec[k] - 2.0 * fdmp5 * g5 * qi * tvj[k] - 2.0 * fdmp5 * g5 * qj * tvi[k];
+            for (int k = 0; k < 3; k++) g[k] += gg[k];
+            dedr += fddr;
+        }
+        // D4 two-body at the output charges (dgw = dgw/dCN)
+        double pe, pg;
+        if (d4_pair(B, spa, B.a_sp[b], r2, pe, pg)) {
+            double c6, da, db;
+            pair_c6(B, S, a, b, c6, da, db);
+            dcn4 -= da * pe;
+            for (int k = 0; k < 3; k++) g[k] += -c6 * pg * v[k];
+        }
+    }
+    for (int k = 0; k < 3; k++) g[k] = warp_sum(g[k]);
+    dedr = warp_sum(dedr);
+    dcn4 = warp_sum(dcn4);
+    if (lane == 0) {
+        for (int k = 0; k < 3; k++) S.grad[3 * a + k] += g[k];
+        S.dedcn[a] += dedr * S.dmrdcn[a];
+        S.dedcn_d4[a] += dcn4;
+    }
+}
+
+// one-electron gradient pieces gathered per atom from the per-pair buffer, plus the on-site CN
+// term (crates/axtb/src/hamiltonian.rs:211-221); warp per atom
+__global__ void k_h0_gather(Batch B, State S, const long long* m_pair0, const double* pairs) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    if (!S.conv[mv.m]) return;
+    int la = a - mv.i0;
+    double g[3] = {0, 0, 0}, dc = 0.0;
+    for (int lb = lane; lb < mv.n; lb += 32) {
+        if (lb == la) continue;
+        if (la > lb) {
+            const double* p = pairs + (m_pair0[mv.m] + (long long)la * (la - 1) / 2 + lb) * 5;
+            for (int k = 0; k < 3; k++) g[k] += p[k];
+            dc += p[3];
+        } else {
+            const double* p = pairs + (m_pair0[mv.m] + (long long)lb * (lb - 1) / 2 + la) * 5;
+            for (int k = 0; k < 3; k++) g[k] -= p[k];
+            dc += p[4];
+        }
+    }
+    for (int k = 0; k < 3; k++) g[k] = warp_sum(g[k]);
+    dc = warp_sum(dc);
+    if (lane == 0) {
+        int n = B.m_nao[mv.m];
+        long long mat = B.m_mat0[mv.m];
+        int ao0 = B.m_ao0[mv.m];
+        for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++)
+            for (int o = B.s_ao0[s]; o < B.s_ao0[s] + 2 * B.s_l[s] + 1; o++) {
+                int mu = o - ao0;
+                dc += S.dsedcn[s] * S.P[mat + mu + (long long)mu * n];
+            }
+        for (int k = 0; k < 3; k++) S.grad[3 * a + k] += g[k];
+        S.dedcn[a] += dc;
+    }
+}
+
+// CN chain rules: GFN2 CN with dE/dCN (crates/base/src/ncoord.rs:486-519) and the D4 CN with
+// its dE/dCN (crates/d4/src/ncoord.rs:56-70); warp per atom
+__global__ void k_cn_chain(Batch B, State S) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    if (!S.conv[mv.m]) return;
+    double g[3] = {0, 0, 0};
+    int spa = B.a_sp[a];
+    for (int b = mv.i0 + lane; b < mv.i0 + mv.n; b += 32) {
+        if (b == a) continue;
+        double v[3];
+        dvec(S.xyz, a, b, v);
+        double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        if (r2 < 1e-12) continue;
+        double r = sqrt(r2);
+        if (r2 <= CN_CUT * CN_CUT) {
+            double d = dexp_dcount(r, B.a_rcov[a] + B.a_rcov[b]);
+            double t = d * (S.dedcn[a] + S.dedcn[b]) / r;
+            for (int k = 0; k < 3; k++) g[k] += t * v[k];
+        }
+        if (r2 <= D4_CN_CUT * D4_CN_CUT) {
+            int spb = B.a_sp[b];
+            double dc = en_factor(B.sp_en[spa], B.sp_en[spb]) * erf_dcount(r, B.sp_rcov[spa] + B.sp_rcov[spb]);
+            double s = S.dedcn_d4[a] + S.dedcn_d4[b];
+            for (int k = 0; k < 3; k++) g[k] += dc * v[k] / r * s;
+        }
+    }
+    for (int k = 0; k < 3; k++) g[k] = warp_sum(g[k]);
+    if (lane == 0)
+        for (int k = 0; k < 3; k++) S.grad[3 * a + k] += g[k];
+}
+
+}  // namespace axg

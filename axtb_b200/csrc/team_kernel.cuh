@@ -1,0 +1,204 @@
+// The cooperative per-molecule dense algebra kernel. Large molecules (team = the whole grid)
+// are processed first, one after the other; then every CTA works through its own list of small
+// molecules (team = that CTA). Phases:
+//   PH_OVERLAP  Cholesky of S and L^-1 (once per geometry; crates/base/src/linalg/eigen.rs:72-113)
+//   PH_EEQ      EEQ start charges from the Cholesky factor of the EEQ matrix
+//               (crates/axtb/src/eeq.rs:43-77, bordered system solved by its Schur complement)
+//   PH_EIGEN    F' = L^-1 F L^-T, eigenvalues, tblite Fermi filling, occupied eigenvectors,
+//               C = L^-T Q Z and P = C f C^T (crates/axtb/src/xtb.rs:997-1038)
+//   PH_WDENS    W = C (f e) C^T (crates/axtb/src/xtb.rs:688-696)
+#pragma once
+#include "common.cuh"
+#include "team_la.cuh"
+
+namespace axg {
+
+enum { PH_OVERLAP = 0, PH_EEQ = 1, PH_EIGEN = 2, PH_WDENS = 3 };
+
+struct TeamPlan {
+    const int* big;        // molecules run by the whole grid
+    int nbig;
+    const int* small_off;  // per CTA: range into small_list
+    const int* small_list;
+    const long long* m_wk0;   // per-molecule workspace offsets into wk
+    double* wk;
+    const long long* m_sq0;   // per-molecule nat^2 offsets (EEQ planes)
+    double* eeq_rhs;          // natT
+    double* eeq_q;            // natT: EEQ charges
+    long long eeq_plane;      // size of one EEQ plane (sum nat^2)
+    int max_chunks;
+};
+
+__device__ void mol_overlap(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+    int n = B.m_nao[m];
+    long long mat = B.m_mat0[m];
+    double* L = S.scr1 + mat;
+    for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) L[e] = S.S[mat + e];
+    t.sync();
+    bool ok = team_cholesky(t, L, n, n);
+    if (!ok && t.tid() == 0) atomicOr(&S.status[m], ST_NOT_PD);
+    double* tmp = P.wk + P.m_wk0[m];
+    team_trinv(t, L, n, S.Linv + mat, n, n, tmp);
+}
+
+__device__ void mol_eeq(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+    int n = B.m_nat[m], a0 = B.m_at0[m];
+    long long o = P.m_sq0[m];
+    double* A = S.eeq_A + o;
+    double* Li = S.eeq_A + P.eeq_plane + o;
+    double* Ji = S.eeq_A + 2 * P.eeq_plane + o;
+    bool ok = team_cholesky(t, A, n, n);
+    double* tmp = P.wk + P.m_wk0[m];
+    team_trinv(t, A, n, Li, n, n, tmp);
+    // J^-1 = L^-T L^-1
+    team_gemm(t, true, false, n, n, n, 1.0, Li, n, Li, n, 0.0, Ji, n);
+    t.sync();
+    // a = J^-1 x, b = J^-1 1 (J^-1 symmetric: row i = column i)
+    double sa = 0.0, sb = 0.0;
+    for (int i = t.tid(); i < n; i += t.nthreads()) {
+        double va = 0.0, vb = 0.0;
+        for (int c = 0; c < n; c++) {
+            double j = Ji[c + (long long)i * n];
+            va += j * P.eeq_rhs[a0 + c];
+            vb += j;
+        }
+        P.eeq_q[a0 + i] = va;
+        tmp[i] = vb;
+        sa += va;
+        sb += vb;
+    }
+    sa = team_sum(t, sa, S.red);
+    sb = team_sum(t, sb, S.red);
+    double lam = (sa - B.m_charge[m]) / sb;
+    for (int i = t.tid(); i < n; i += t.nthreads()) {
+        double q = P.eeq_q[a0 + i] - lam * tmp[i];
+        if (!ok || !isfinite(q)) q = 0.0;  // neutral-atom start when the EEQ system fails
+        P.eeq_q[a0 + i] = q;
+    }
+    t.sync();
+}
+
+__device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+    int n = B.m_nao[m], ao0 = B.m_ao0[m];
+    long long mat = B.m_mat0[m];
+    double* wk = P.wk + P.m_wk0[m];
+    double* Linv = S.Linv + mat;
+    double* X = S.scr1 + mat;
+    double* Fp = S.Fp + mat;
+    // F' = L^-1 F L^-T, symmetrised
+    team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n);
+    t.sync();
+    team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n);
+    t.sync();
+    for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) {
+        int i = (int)(e % n), c = (int)(e / n);
+        if (i > c) {
+            double v = 0.5 * (Fp[i + (long long)c * n] + Fp[c + (long long)i * n]);
+            Fp[i + (long long)c * n] = v;
+            Fp[c + (long long)i * n] = v;
+        }
+    }
+    t.sync();
+    double* d = S.dtri + ao0;
+    double* e = S.etri + ao0;
+    double* tau = S.tau + ao0;
+    double* vbuf = wk;
+    double* pbuf = wk + n;
+    double* ppart = wk + 2 * n;
+    team_tridiag(t, Fp, n, n, d, e, tau, vbuf, pbuf, ppart, S.red, P.max_chunks);
+    double* emo = S.emo + ao0;
+    team_bisect(t, d, e, n, emo, wk);
+    // Fermi filling of both spins (warp 0 of CTA 0), kocc and -TS
+    double* focc = S.focc + ao0;
+    double* occb = wk + 8;  // n entries
+    if (t.rank == 0 && threadIdx.x < 32) {
+        double efa, efb;
+        warp_fill(B.m_nalpha[m], B.kt, emo, n, focc, &efa);
+        warp_fill(B.m_nbeta[m], B.kt, emo, n, occb, &efb);
+        int lane = threadIdx.x;
+        double pa = 0.0, pb = 0.0, ts = 0.0;
+        int kl = 0;
+        for (int i = lane; i < n; i += 32) {
+            double fa = focc[i], fb = occb[i];
+            pa += fa;
+            pb += fb;
+            if (B.kt > 0.0) ts += log(pow(fa, fa) * pow(1.0 - fa, 1.0 - fa)) + log(pow(fb, fb) * pow(1.0 - fb, 1.0 - fb));
+            double f = fa + fb;
+            focc[i] = f;
+            if (f > 1e-16) kl = max(kl, i + 1);
+        }
+        pa = warp_sum(pa);
+        pb = warp_sum(pb);
+        ts = warp_sum(ts);
+        for (int o = 16; o > 0; o >>= 1) kl = max(kl, __shfl_xor_sync(0xffffffffu, kl, o));
+        if (lane == 0) {
+            S.kocc[m] = kl;
+            S.ts[m] = ts * B.kt;
+            if (fabs(pa - B.m_nalpha[m]) > 1e-6 || fabs(pb - B.m_nbeta[m]) > 1e-6) atomicOr(&S.status[m], ST_FERMI);
+        }
+    }
+    t.sync();
+    int k = S.kocc[m];
+    double* Zm = S.Z + mat;
+    team_invit(t, d, e, emo, n, k, Zm, n, S.scr1 + mat, S.scr2 + mat, S.scr3 + mat, S.piv + mat, S.P + mat, &S.status[m]);
+    // back-transform: vb (n x 64), tb, gm (64 x 64), y, y2 (64 x k)
+    double* vb = wk + 2 * n + (long long)P.max_chunks * n;
+    double* tb = vb + 64LL * n;
+    double* gm = tb + 64 * 64;
+    double* y = gm + 64 * 64;
+    double* y2 = y + 64LL * n;
+    team_backtransform(t, Fp, n, tau, n, k, Zm, n, vb, tb, gm, y, y2);
+    // C = L^-T Z'; P = (C f) C^T
+    double* Cm = S.C + mat;
+    team_gemm(t, true, false, n, k, n, 1.0, Linv, n, Zm, n, 0.0, Cm, n);
+    t.sync();
+    double* Cf = S.scr1 + mat;
+    for (long long q = t.tid(); q < (long long)n * k; q += t.nthreads()) Cf[q] = Cm[q] * focc[q / n];
+    t.sync();
+    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.P + mat, n);
+    t.sync();
+}
+
+__device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+    int n = B.m_nao[m], ao0 = B.m_ao0[m], k = S.kocc[m];
+    long long mat = B.m_mat0[m];
+    double* Cm = S.C + mat;
+    double* Cf = S.scr1 + mat;
+    for (long long q = t.tid(); q < (long long)n * k; q += t.nthreads()) {
+        int c = (int)(q / n);
+        Cf[q] = Cm[q] * (S.focc[ao0 + c] * S.emo[ao0 + c]);
+    }
+    t.sync();
+    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.W + mat, n);
+    t.sync();
+}
+
+__device__ __forceinline__ bool phase_wants(const State& S, int phase, int m) {
+    if (phase == PH_EIGEN) return S.active[m] != 0;
+    if (phase == PH_WDENS) return S.conv[m] != 0;
+    return true;
+}
+
+__device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan& P, int phase, int m) {
+    switch (phase) {
+        case PH_OVERLAP: mol_overlap(t, B, S, P, m); break;
+        case PH_EEQ: mol_eeq(t, B, S, P, m); break;
+        case PH_EIGEN: mol_eigen(t, B, S, P, m); break;
+        case PH_WDENS: mol_wdens(t, B, S, P, m); break;
+    }
+}
+
+__global__ void __launch_bounds__(TEAM_THREADS) k_team(Batch B, State S, TeamPlan P, int phase) {
+    Team g{(int)blockIdx.x, (int)gridDim.x, true};
+    for (int i = 0; i < P.nbig; i++) {
+        int m = P.big[i];
+        if (phase_wants(S, phase, m)) run_mol(g, B, S, P, phase, m);  // uniform across the grid
+    }
+    Team one{0, 1, false};
+    for (int i = P.small_off[blockIdx.x]; i < P.small_off[blockIdx.x + 1]; i++) {
+        int m = P.small_list[i];
+        if (phase_wants(S, phase, m)) run_mol(one, B, S, P, phase, m);
+    }
+}
+
+}  // namespace axg

@@ -1,0 +1,546 @@
+// Dense FP64 linear algebra run by a "team": one CTA (small molecules, many per launch, each CTA
+// taking its own molecules) or the whole cooperative grid (a large molecule, every CTA at once).
+// The same device functions serve both; a team barrier is __syncthreads() for one CTA and a
+// grid-wide barrier for the whole grid (cooperative launch, so every CTA is resident).
+//
+// Matrices are column-major with an explicit leading dimension. These routines compute the
+// quantities of the reference's dense algebra (crates/base/src/linalg/eigen.rs: Cholesky of S,
+// the reduced matrix L^-1 F L^-T, its eigenvalues and occupied eigenvectors, C = L^-T U; and
+// crates/base/src/linalg/density.rs: P = C diag(f) C^T) with B200-friendly algorithms:
+// right-looking Cholesky, a row-block triangular inverse on GEMMs, Householder
+// tridiagonalisation with 2-D split symmetric matrix-vector products, Sturm-count bisection for
+// all eigenvalues (one thread per eigenvalue), inverse iteration for the occupied vectors (one
+// thread per vector, re-orthogonalised within clusters of close eigenvalues) and the blocked
+// (compact WY) back-transformation on GEMMs.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+
+namespace axg {
+namespace cg = cooperative_groups;
+
+constexpr int TEAM_THREADS = 256;
+
+struct Team {
+    int rank;     // CTA rank in the team
+    int size;     // CTAs in the team
+    bool global;  // the team is the whole grid
+    __device__ __forceinline__ void sync() const {
+        if (global) cg::this_grid().sync();
+        else __syncthreads();
+    }
+    __device__ __forceinline__ int tid() const { return rank * blockDim.x + threadIdx.x; }
+    __device__ __forceinline__ int nthreads() const { return size * blockDim.x; }
+    __device__ __forceinline__ int warp() const { return (rank * blockDim.x + threadIdx.x) >> 5; }
+    __device__ __forceinline__ int nwarps() const { return (size * blockDim.x) >> 5; }
+};
+
+// Deterministic team sum: warp sums, CTA sum in fixed warp order, then (global team) the CTA
+// partials summed in rank order by every thread. `gred` holds one double per CTA.
+__device__ double team_sum(const Team& t, double v, double* gred) {
+    __shared__ double sred[TEAM_THREADS / 32];
+    __shared__ double sout;
+    v = warp_sum(v);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sred[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sred[k];
+        sout = s;
+    }
+    __syncthreads();
+    double blk = sout;
+    if (!t.global) return blk;
+    if (threadIdx.x == 0) gred[t.rank] = blk;
+    t.sync();
+    double s = 0.0;
+    for (int k = 0; k < t.size; k++) s += gred[k];
+    t.sync();  // gred reusable afterwards
+    return s;
+}
+
+// ---------------------------------------------------------------------------------- GEMM
+// C(MxN) = alpha op(A) op(B) + beta C; op(A) = A (M x K, lda) or A^T (A is K x M);
+// op(B) = B (K x N, ldb) or B^T (B is N x K). 64x64 tiles, k-steps of 16, 4x4 per thread.
+constexpr int GT = 64, GK = 16;
+
+__device__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
+                          long long lda, const double* B, long long ldb, double beta, double* Cm, long long ldc) {
+    __shared__ double As[GK][GT + 1];
+    __shared__ double Bs[GK][GT + 1];
+    if (M <= 0 || N <= 0) return;
+    int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
+    int r = threadIdx.x & 15, c = threadIdx.x >> 4;
+    for (int tile = t.rank; tile < tm * tn; tile += t.size) {
+        int bi = tile % tm, bj = tile / tm;
+        int row0 = bi * GT, col0 = bj * GT;
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+        for (int k0 = 0; k0 < K; k0 += GK) {
+            __syncthreads();
+            for (int e = threadIdx.x; e < GT * GK; e += blockDim.x) {
+                int kk, mm;
+                if (!ta) {
+                    mm = e % GT;
+                    kk = e / GT;
+                } else {
+                    kk = e % GK;
+                    mm = e / GK;
+                }
+                int gr = row0 + mm, gk = k0 + kk;
+                double v = 0.0;
+                if (gr < M && gk < K) v = ta ? A[gk + (long long)gr * lda] : A[gr + (long long)gk * lda];
+                As[kk][mm] = v;
+            }
+            for (int e = threadIdx.x; e < GT * GK; e += blockDim.x) {
+                int kk, nn;
+                if (!tb) {
+                    kk = e % GK;
+                    nn = e / GK;
+                } else {
+                    nn = e % GT;
+                    kk = e / GT;
+                }
+                int gc = col0 + nn, gk = k0 + kk;
+                double v = 0.0;
+                if (gc < N && gk < K) v = tb ? B[gc + (long long)gk * ldb] : B[gk + (long long)gc * ldb];
+                Bs[kk][nn] = v;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < GK; kk++) {
+                double a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i] = As[kk][r + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; j++) b[j] = Bs[kk][c + 16 * j];
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            int gc = col0 + c + 16 * j;
+            if (gc >= N) continue;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                int gr = row0 + r + 16 * i;
+                if (gr >= M) continue;
+                double* dst = &Cm[gr + (long long)gc * ldc];
+                double v = alpha * acc[i][j];
+                *dst = beta == 0.0 ? v : v + beta * *dst;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------- Cholesky
+// In-place lower Cholesky of the n x n SPD matrix A (the strict upper triangle is zeroed).
+// Returns false (on every thread) when a pivot is not positive.
+__device__ bool team_cholesky(const Team& t, double* A, int n, long long lda) {
+    bool ok = true;
+    for (int j = 0; j < n; j++) {
+        double ajj = A[j + (long long)j * lda];
+        if (!(ajj > 0.0)) {
+            ok = false;
+            ajj = 1.0;
+        }
+        double ljj = sqrt(ajj);
+        double inv = 1.0 / ljj;
+        for (int i = j + 1 + t.tid(); i < n; i += t.nthreads()) A[i + (long long)j * lda] *= inv;
+        t.sync();
+        if (t.tid() == 0) A[j + (long long)j * lda] = ljj;
+        int m = n - j - 1;
+        long long tot = (long long)m * m;
+        for (long long e = t.tid(); e < tot; e += t.nthreads()) {
+            int i = j + 1 + (int)(e % m), c = j + 1 + (int)(e / m);
+            if (i < c) continue;
+            A[i + (long long)c * lda] -= A[i + (long long)j * lda] * A[c + (long long)j * lda];
+        }
+        t.sync();
+    }
+    for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) {
+        int i = (int)(e % n), c = (int)(e / n);
+        if (i < c) A[i + (long long)c * lda] = 0.0;
+    }
+    t.sync();
+    return ok;
+}
+
+// Linv = L^-1 for lower triangular L (n x n), row blocks of 64: Linv[I, :] = L_II^-1 (E_I -
+// L[I, 0:i0] Linv[0:i0, :]); `tmp` holds 64 x n.
+__device__ void team_trinv(const Team& t, const double* L, long long ldl, double* Linv, long long ldi, int n, double* tmp) {
+    for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) Linv[(e % n) + (e / n) * ldi] = 0.0;
+    t.sync();
+    for (int i0 = 0; i0 < n; i0 += GT) {
+        int nb = min(GT, n - i0), i1 = i0 + nb;
+        // tmp (nb x i1) = -L[I, 0:i0] Linv[0:i0, 0:i1]
+        if (i0 > 0) team_gemm(t, false, false, nb, i1, i0, -1.0, L + i0, ldl, Linv, ldi, 0.0, tmp, GT);
+        else
+            for (long long e = t.tid(); e < (long long)nb * i1; e += t.nthreads()) tmp[(e % nb) + (e / nb) * GT] = 0.0;
+        t.sync();
+        // solve L_II X = tmp + E for each column c < i1 (one thread per column)
+        for (int c = t.tid(); c < i1; c += t.nthreads()) {
+            for (int r = 0; r < nb; r++) {
+                double v = tmp[r + (long long)c * GT] + ((i0 + r) == c ? 1.0 : 0.0);
+                for (int q = 0; q < r; q++) v -= L[(i0 + r) + (long long)(i0 + q) * ldl] * tmp[q + (long long)c * GT];
+                v /= L[(i0 + r) + (long long)(i0 + r) * ldl];
+                tmp[r + (long long)c * GT] = v;
+            }
+            for (int r = 0; r < nb; r++) Linv[(i0 + r) + (long long)c * ldi] = (c <= i0 + r) ? tmp[r + (long long)c * GT] : 0.0;
+        }
+        t.sync();
+    }
+}
+
+// ---------------------------------------------------------------------------------- tridiagonal
+// Householder reduction of the symmetric A (full storage, n x n) to T = Q^T A Q; d, e get the
+// diagonal and subdiagonal, tau the reflector factors; reflector j (I - tau_j v v^T, v_{j+1} = 1)
+// is kept in A[j+2:n, j]. vbuf/pbuf hold n doubles; ppart holds nchunk*n partial sums.
+__device__ void team_tridiag(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
+                             double* vbuf, double* pbuf, double* ppart, double* gred, int max_chunks) {
+    for (int j = 0; j + 2 < n; j++) {
+        int r0 = j + 1, m = n - r0;  // trailing block rows/cols r0..n-1
+        double alpha = A[r0 + (long long)j * lda];
+        double xs = 0.0;
+        for (int i = r0 + 1 + t.tid(); i < n; i += t.nthreads()) xs += sq(A[i + (long long)j * lda]);
+        double xnorm2 = team_sum(t, xs, gred);
+        double beta, tj, scale;
+        if (xnorm2 == 0.0) {
+            tj = 0.0;
+            beta = alpha;
+            scale = 0.0;
+        } else {
+            beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+            tj = (beta - alpha) / beta;
+            scale = 1.0 / (alpha - beta);
+        }
+        for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
+            double v = i == r0 ? 1.0 : A[i + (long long)j * lda] * scale;
+            vbuf[i] = v;
+            if (i > r0) A[i + (long long)j * lda] = v;
+        }
+        if (t.tid() == 0) {
+            e[j] = beta;
+            tau[j] = tj;
+            d[j] = A[j + (long long)j * lda];
+            A[r0 + (long long)j * lda] = beta;
+        }
+        t.sync();
+        if (tj != 0.0) {
+            // p = tau A v over the trailing block: warps own 32-row tiles x column chunks
+            int rt = (m + 31) / 32;
+            int nch = max(1, min(max_chunks, (t.nwarps() * 2 + rt - 1) / rt));
+            int cw = (m + nch - 1) / nch;
+            int lane = threadIdx.x & 31;
+            for (int it = t.warp(); it < rt * nch; it += t.nwarps()) {
+                int tr = it % rt, ch = it / rt;
+                int row = r0 + tr * 32 + lane;
+                int c0 = r0 + ch * cw, c1 = min(n, c0 + cw);
+                double s = 0.0;
+                if (row < n)
+                    for (int c = c0; c < c1; c++) s = fma(A[row + (long long)c * lda], vbuf[c], s);
+                if (row < n) ppart[(long long)ch * n + row] = s;
+            }
+            t.sync();
+            double pv = 0.0;
+            for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
+                double s = 0.0;
+                for (int ch = 0; ch < nch; ch++) s += ppart[(long long)ch * n + i];
+                s *= tj;
+                pbuf[i] = s;
+                pv += s * vbuf[i];
+            }
+            double dot = team_sum(t, pv, gred);
+            double K = -0.5 * tj * dot;
+            for (int i = r0 + t.tid(); i < n; i += t.nthreads()) pbuf[i] += K * vbuf[i];  // w
+            t.sync();
+            long long tot = (long long)m * m;
+            for (long long q = t.tid(); q < tot; q += t.nthreads()) {
+                int i = r0 + (int)(q % m), c = r0 + (int)(q / m);
+                A[i + (long long)c * lda] -= vbuf[i] * pbuf[c] + pbuf[i] * vbuf[c];
+            }
+            t.sync();
+        }
+    }
+    if (t.tid() == 0) {
+        if (n >= 2) {
+            d[n - 2] = A[(n - 2) + (long long)(n - 2) * lda];
+            e[n - 2] = A[(n - 1) + (long long)(n - 2) * lda];
+            tau[n - 2] = 0.0;
+        }
+        d[n - 1] = A[(n - 1) + (long long)(n - 1) * lda];
+        e[n - 1] = 0.0;
+        tau[n - 1] = 0.0;
+    }
+    t.sync();
+}
+
+// number of eigenvalues of the symmetric tridiagonal (d, e) below x (Sturm sequence)
+__device__ __forceinline__ int sturm_count(const double* d, const double* e, int n, double x, double pivmin) {
+    int cnt = 0;
+    double q = d[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    if (q < 0.0) cnt++;
+    for (int i = 1; i < n; i++) {
+        q = d[i] - x - e[i - 1] * e[i - 1] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        if (q < 0.0) cnt++;
+    }
+    return cnt;
+}
+
+// all eigenvalues (ascending) by bisection, one thread per eigenvalue index
+__device__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w, double* gbuf) {
+    // gbuf[0..2]: Gershgorin bounds and pivmin (computed by thread 0 of the team)
+    if (t.tid() == 0) {
+        double lo = INFINITY, hi = -INFINITY, emax = 0.0;
+        for (int i = 0; i < n; i++) {
+            double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+            lo = fmin(lo, d[i] - r);
+            hi = fmax(hi, d[i] + r);
+            if (i + 1 < n) emax = fmax(emax, e[i] * e[i]);
+        }
+        double tnrm = fmax(fabs(lo), fabs(hi));
+        lo -= 2.0 * DBL_EPSILON * tnrm * n + 1e-300;
+        hi += 2.0 * DBL_EPSILON * tnrm * n + 1e-300;
+        gbuf[0] = lo;
+        gbuf[1] = hi;
+        gbuf[2] = DBL_MIN * fmax(1.0, emax);
+    }
+    t.sync();
+    double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
+    for (int k = t.tid(); k < n; k += t.nthreads()) {
+        double lo = glo, hi = ghi;
+        for (int it = 0; it < 200; it++) {
+            double mid = 0.5 * (lo + hi);
+            if (hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin || mid <= lo || mid >= hi) break;
+            if (sturm_count(d, e, n, mid, pivmin) > k) hi = mid;
+            else lo = mid;
+        }
+        w[k] = 0.5 * (lo + hi);
+    }
+    t.sync();
+}
+
+// ---------------------------------------------------------------------------------- Fermi
+// tblite Fermi filling of nel electrons at kT over the ascending levels emo (one warp):
+// crates/base/src/occupations.rs:58-128; returns false when kt == 0 (aufbau only).
+__device__ void warp_fill(double nel, double kt, const double* emo, int n, double* occ, double* ef_out) {
+    int lane = threadIdx.x & 31;
+    int full = (int)floor(nel);
+    double rem = fmod(nel, 1.0);
+    for (int i = lane; i < n; i += 32) occ[i] = i < full ? 1.0 : (i == full ? rem : 0.0);
+    int homo = full + (rem > 0.5 ? 1 : 0);
+    __syncwarp();
+    if (!(nel > 0.0 && kt > 0.0)) {
+        *ef_out = 0.0;
+        return;
+    }
+    int i0 = max(homo, 1) - 1, i1 = min(homo + 1, n) - 1;
+    double ef = 0.5 * (emo[i0] + emo[i1]), ef_used = ef;
+    const double tol = 1e5 * DBL_EPSILON, sqrttiny = sqrt(DBL_MIN);
+    for (int it = 0; it < 200; it++) {
+        double tot = 0.0, dtot = 0.0;
+        ef_used = ef;
+        for (int i = lane; i < n; i += 32) {
+            double arg = (emo[i] - ef) / kt, f, df;
+            if (arg > 50.0) {
+                f = 0.0;
+                df = 0.0;
+            } else if (arg < -50.0) {
+                f = 1.0;
+                df = 0.0;
+            } else {
+                f = 1.0 / (exp(arg) + 1.0);
+                df = -f * (1.0 - f) / kt;
+            }
+            occ[i] = f;
+            tot += f;
+            dtot -= df;
+        }
+        tot = warp_sum(tot);
+        dtot = warp_sum(dtot);
+        if (fabs(nel - tot) <= tol) break;
+        if (dtot > sqrttiny) ef += (nel - tot) / dtot;
+        else break;
+    }
+    __syncwarp();
+    *ef_out = ef_used;
+}
+
+// ---------------------------------------------------------------------------------- inverse iteration
+__device__ __forceinline__ double hash_uniform(unsigned int a, unsigned int b) {
+    unsigned int h = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return ((double)h / 4294967296.0) * 2.0 - 1.0;
+}
+
+// Eigenvectors of the tridiagonal (d, e) for the eigenvalues w[0..k) by inverse iteration, one
+// thread per cluster of eigenvalues closer than ctol (vectors of a cluster re-orthogonalised
+// against its earlier members). Vector q is written to column q of V (n x k, ldv). Work planes
+// u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved).
+// Returns (through flag) nonzero when a vector was not finite.
+__device__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
+                           double* V, long long ldv, double* u0, double* u1, double* lm, unsigned char* piv, double* x,
+                           int* flag) {
+    double tnrm = 0.0;
+    for (int i = 0; i < n; i++) {
+        double r = fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+        tnrm = fmax(tnrm, r);
+    }
+    if (tnrm == 0.0) tnrm = 1.0;
+    const double ctol = 1e-6 * tnrm, pert = 10.0 * DBL_EPSILON * tnrm, pivmin = DBL_EPSILON * tnrm;
+    const long long LD = n;  // interleave stride
+    for (int q0 = t.tid(); q0 < k; q0 += t.nthreads()) {
+        if (q0 > 0 && w[q0] - w[q0 - 1] <= ctol) continue;  // not a cluster head
+        int q1 = q0 + 1;
+        while (q1 < k && w[q1] - w[q1 - 1] <= ctol) q1++;
+        double lam_prev = -INFINITY;
+        for (int q = q0; q < q1; q++) {
+            double lam = w[q];
+            if (q > q0 && lam < lam_prev + pert) lam = lam_prev + pert;
+            lam_prev = lam;
+            // LU with partial pivoting of T - lam I; active row (ca, cb)
+            double ca = d[0] - lam, cb = n > 1 ? e[0] : 0.0;
+            for (int i = 0; i + 1 < n; i++) {
+                double sub = e[i], a1 = d[i + 1] - lam, b1 = (i + 2 < n) ? e[i + 1] : 0.0;
+                long long ix = (long long)i * LD + q;
+                if (fabs(ca) >= fabs(sub)) {
+                    double p = ca;
+                    if (p == 0.0) p = pivmin;
+                    double l = sub / p;
+                    u0[ix] = p;
+                    u1[ix] = cb;
+                    lm[ix] = l;
+                    piv[ix] = 0;
+                    ca = a1 - l * cb;
+                    cb = b1;
+                } else {
+                    double l = ca / sub;
+                    u0[ix] = sub;
+                    u1[ix] = a1;
+                    lm[ix] = l;
+                    piv[ix] = 1;
+                    ca = cb - l * a1;
+                    cb = -l * b1;
+                }
+            }
+            {
+                long long ix = (long long)(n - 1) * LD + q;
+                u0[ix] = (ca == 0.0) ? pivmin : ca;
+            }
+            for (int i = 0; i < n; i++) x[(long long)i * LD + q] = hash_uniform((unsigned)q, (unsigned)i);
+            for (int iter = 0; iter < 3; iter++) {
+                // forward: L with the row interchanges
+                for (int i = 0; i + 1 < n; i++) {
+                    long long ix = (long long)i * LD + q, ix1 = ix + LD;
+                    double xi = x[ix], xi1 = x[ix1];
+                    if (piv[ix]) {
+                        double tmp = xi;
+                        xi = xi1;
+                        xi1 = tmp;
+                        x[ix] = xi;
+                    }
+                    x[ix1] = xi1 - lm[ix] * xi;
+                }
+                // backward: U with up to two superdiagonals (u2_i = e_{i+1} after an interchange)
+                double xn1 = 0.0, xn2 = 0.0;
+                for (int i = n - 1; i >= 0; i--) {
+                    long long ix = (long long)i * LD + q;
+                    double v = x[ix];
+                    if (i + 1 < n) v -= u1[ix] * xn1;
+                    if (i + 2 < n && piv[ix]) v -= e[i + 1] * xn2;
+                    v /= u0[ix];
+                    x[ix] = v;
+                    xn2 = xn1;
+                    xn1 = v;
+                }
+                // scale by the largest element, orthogonalise within the cluster, normalise
+                double mx = 0.0;
+                for (int i = 0; i < n; i++) mx = fmax(mx, fabs(x[(long long)i * LD + q]));
+                if (!(mx > 0.0) || !isfinite(mx)) {
+                    atomicOr(flag, ST_INVIT);
+                    mx = 1.0;
+                }
+                double inv = 1.0 / mx;
+                for (int i = 0; i < n; i++) x[(long long)i * LD + q] *= inv;
+                for (int p = q0; p < q; p++) {
+                    double dt = 0.0;
+                    for (int i = 0; i < n; i++) dt += x[(long long)i * LD + p] * x[(long long)i * LD + q];
+                    for (int i = 0; i < n; i++) x[(long long)i * LD + q] -= dt * x[(long long)i * LD + p];
+                }
+                double nr = 0.0;
+                for (int i = 0; i < n; i++) nr += sq(x[(long long)i * LD + q]);
+                nr = 1.0 / sqrt(nr);
+                for (int i = 0; i < n; i++) x[(long long)i * LD + q] *= nr;
+            }
+            for (int i = 0; i < n; i++) V[i + (long long)q * ldv] = x[(long long)i * LD + q];
+        }
+    }
+    t.sync();
+}
+
+// Z <- Q Z for Q = H_0 H_1 ... H_{n-3} kept in A (team_tridiag), Z = V (n x k, ldv), blocked by
+// 64 reflectors (compact WY: H_b..H_{b+nb-1} = I - Vb T Vb^T, T upper triangular).
+// Work: vb (n x 64), tb (64 x 64), gm (64 x 64), y (64 x k), y2 (64 x k).
+__device__ void team_backtransform(const Team& t, const double* A, long long lda, const double* tau, int n, int k,
+                                   double* V, long long ldv, double* vb, double* tb, double* gm, double* y, double* y2) {
+    int nrefl = n - 2;
+    if (nrefl <= 0 || k <= 0) return;
+    const int NB = GT;
+    for (int b0 = ((nrefl - 1) / NB) * NB; b0 >= 0; b0 -= NB) {
+        int jb = min(NB, nrefl - b0);
+        int r0 = b0 + 1, nr = n - r0;
+        // explicit Vb (nr x jb, ld nr): unit at row c, A below, zero above
+        for (long long q = t.tid(); q < (long long)nr * jb; q += t.nthreads()) {
+            int r = (int)(q % nr), c = (int)(q / nr);
+            double v = r == c ? 1.0 : (r > c ? A[(r0 + r) + (long long)(b0 + c) * lda] : 0.0);
+            vb[r + (long long)c * nr] = v;
+        }
+        t.sync();
+        // G = Vb^T Vb (jb x jb)
+        team_gemm(t, true, false, jb, jb, nr, 1.0, vb, nr, vb, nr, 0.0, gm, NB);
+        t.sync();
+        // T by the forward recurrence (one warp of CTA 0)
+        if (t.rank == 0 && threadIdx.x < 32) {
+            int lane = threadIdx.x;
+            for (int q = lane; q < NB * NB; q += 32) tb[q] = 0.0;
+            __syncwarp();
+            for (int c = 0; c < jb; c++) {
+                double tc = tau[b0 + c];
+                // column c: T[0:c, c] = -tau_c T[0:c,0:c] G[0:c, c]
+                for (int i = lane; i < c; i += 32) {
+                    double s = 0.0;
+                    for (int q = i; q < c; q++) s += tb[i + q * NB] * gm[q + c * NB];
+                    tb[i + c * NB] = -tc * s;
+                }
+                __syncwarp();
+                if (lane == 0) tb[c + c * NB] = tc;
+                __syncwarp();
+            }
+        }
+        t.sync();
+        // y = Vb^T Z[r0:, :] (jb x k); y2 = T y; Z[r0:, :] -= Vb y2
+        team_gemm(t, true, false, jb, k, nr, 1.0, vb, nr, V + r0, ldv, 0.0, y, NB);
+        t.sync();
+        team_gemm(t, false, false, jb, k, jb, 1.0, tb, NB, y, NB, 0.0, y2, NB);
+        t.sync();
+        team_gemm(t, false, false, nr, k, jb, -1.0, vb, nr, y2, NB, 1.0, V + r0, ldv);
+        t.sync();
+    }
+}
+
+}  // namespace axg

@@ -1,0 +1,136 @@
+/* axtb_gpu.h - C ABI of the B200 (sm_100a) GFN2-xTB energy + gradient engine.
+ *
+ * Drop-in boundary for axtb's GFN2-xTB single point. The reference interface each entry point
+ * replaces (paths in the axtb repository):
+ *
+ *   axtb_gpu_create       axtb::Calculator::new(Hamiltonian::Gfn2, numbers, positions, charge,
+ *                         uhf, Options) -- crates/axtb/src/calculator.rs:92-128, with the
+ *                         molecule checks of crates/base/src/molecule.rs:35-60 and the SCF
+ *                         option checks of crates/axtb/src/xtb.rs:1159-1174
+ *   axtb_gpu_singlepoint  Method::singlepoint(&mut self, positions, &Want) --
+ *                         crates/base/src/method/mod.rs:62, impl crates/axtb/src/calculator.rs:387-395
+ *                         (the warm start from the previous geometry's moments,
+ *                         calculator.rs:194-206), returning the SinglePoint fields of
+ *                         crates/base/src/method/results.rs:39-57
+ *   axtb_gpu_batch        no reference counterpart (axtb runs one calculation per process or
+ *                         per Session lineage, crates/driver/src/calculator.rs:258-277): many
+ *                         independent single points in one device pass
+ *   axtb_gpu_destroy      Drop of the calculator
+ *   axtb_gpu_last_error   the message of crates/base/src/error.rs:8-24 Error values
+ *
+ * Status codes mirror the reference's Error kinds (crates/base/src/error.rs:8-24).
+ * Nothing here aborts, traps or hangs: device loops are bounded by max_iter and report a
+ * status. All pointers are host pointers unless stated; outputs are caller-allocated and no
+ * pointer is retained after a call returns. A handle is used by one thread at a time.
+ */
+#ifndef AXTB_GPU_H
+#define AXTB_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum AxtbStatus {
+    AXTB_OK = 0,
+    AXTB_ERR_INPUT = 1,               /* Error::Input */
+    AXTB_ERR_UNSUPPORTED_ELEMENT = 2, /* Error::UnsupportedElement */
+    AXTB_ERR_SCF_NOT_CONVERGED = 3,   /* Error::ScfNotConverged {iterations, energy_change, residual} */
+    AXTB_ERR_NUMERICAL = 4,           /* Error::Numerical (non-finite values, lost Fermi level, ...) */
+    AXTB_ERR_DEVICE = 5,              /* CUDA error or missing device (no CPU fallback exists) */
+};
+
+/* Options (crates/axtb/src/lib.rs:92-133 Options and ScfSettings; defaults of
+ * crates/axtb/src/xtb.rs:101-106). Fill with axtb_gpu_default_options. */
+typedef struct AxtbOptions {
+    double accuracy;   /* SCF accuracy multiplier (thresholds 1e-6*acc Eh and 2e-5*acc e); 1.0 */
+    double etemp;      /* electronic temperature, K; 300 */
+    int32_t max_iter;  /* iterations of the SCF; 250 */
+    double damping;    /* Broyden damping, (0, 1]; 0.4 */
+    int32_t guess;     /* 0: EEQ charges (default), 1: neutral atoms */
+    int32_t precision; /* 0: FP64 throughout (default); 1: split precision (3xBF16 dense products) */
+    int32_t device;    /* CUDA device ordinal; 0 */
+} AxtbOptions;
+
+/* Results of one single point (crates/base/src/method/results.rs:39-57). Array members are
+ * caller-allocated and may be NULL when not wanted. */
+typedef struct AxtbResult {
+    double energy;          /* total energy, Eh */
+    double* gradient;       /* nat*3, Eh/bohr (written when the gradient is requested) */
+    double* charges;        /* nat Mulliken atomic charges */
+    double* dipole;         /* 3, e*bohr */
+    double* qsh;            /* nsh shell charges */
+    double* dpat;           /* nat*3 atomic dipoles */
+    double* qpat;           /* nat*6 atomic quadrupoles (xx, xy, yy, xz, yz, zz) */
+    double terms[8];        /* repulsion, dispersion, electronic, isotropic_es, third_order,
+                               anisotropic, entropy, band */
+    int32_t iterations;     /* SCF iterations */
+    int32_t converged;      /* 1 when converged */
+    int32_t status;         /* AxtbStatus of this molecule */
+    double energy_change;   /* last |dE| (ScfNotConverged payload) */
+    double residual;        /* last residual norm (ScfNotConverged payload) */
+} AxtbResult;
+
+/* One molecule of a batch: atomic numbers, positions (bohr, nat*3 row-major), charge and the
+ * number of unpaired electrons (-1 for the default, nel mod 2). */
+typedef struct AxtbMol {
+    int32_t nat;
+    const int32_t* numbers;
+    const double* positions;
+    double charge;
+    int32_t uhf;
+} AxtbMol;
+
+typedef struct AxtbHandle AxtbHandle;
+typedef struct AxtbBatch AxtbBatch;
+
+void axtb_gpu_default_options(AxtbOptions* opts);
+
+/* Sizes of a molecule's basis (shells and AOs); AXTB_ERR_UNSUPPORTED_ELEMENT past Rn. */
+int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao);
+
+/* Calculator for one molecule (axtb::Calculator::new). The positions set the first geometry
+ * checked; singlepoint takes the positions of each call. */
+int axtb_gpu_create(const int32_t* numbers, int32_t nat, double charge, int32_t uhf, const AxtbOptions* opts,
+                    AxtbHandle** out);
+
+/* E (+ gradient when want_gradient) at `positions` (host, bohr, nat*3). The SCF starts from the
+ * previous call's converged moments when there is one, and once more from the EEQ guess when
+ * that start fails (crates/axtb/src/calculator.rs:194-206). */
+int axtb_gpu_singlepoint(AxtbHandle* h, const double* positions, int32_t want_gradient, AxtbResult* out);
+
+void axtb_gpu_destroy(AxtbHandle* h);
+
+/* Message of the last failed call on `h` (or of the last failed handle-less call when h is
+ * NULL); returns the message length. */
+int axtb_gpu_last_error(const AxtbHandle* h, char* buf, size_t len);
+
+/* Many independent single points in one device pass. `outs[i]` receives molecule i's results,
+ * `status[i]` its AxtbStatus (also outs[i].status). Returns AXTB_OK when the pass ran (per-
+ * molecule failures are reported in status), an error code otherwise. */
+int axtb_gpu_batch(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, int32_t want_gradient,
+                   AxtbResult* outs, int32_t* status);
+
+/* Reusable batch: set up once for a list of molecules (their numbers, charges, spins and a
+ * first geometry), then run it on new positions. axtb_gpu_batch_run takes host positions
+ * (all molecules' nat*3 arrays concatenated in batch order); axtb_gpu_batch_run_device takes
+ * a DEVICE pointer to the same layout and writes energies (nmol) and, with want_gradient,
+ * gradients (same layout as the positions) to DEVICE pointers, on the batch's stream. */
+int axtb_gpu_batch_create(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, AxtbBatch** out);
+int axtb_gpu_batch_run(AxtbBatch* b, const double* positions, int32_t want_gradient, AxtbResult* outs,
+                       int32_t* status);
+int axtb_gpu_batch_run_device(AxtbBatch* b, const double* d_positions, int32_t want_gradient, double* d_energy,
+                              double* d_gradient, int32_t* status);
+/* The CUDA stream (cudaStream_t) the batch runs on, for callers that time or order work. */
+void* axtb_gpu_batch_stream(AxtbBatch* b);
+/* Number of kernels the last run launched (counted on the host at each launch). */
+int64_t axtb_gpu_batch_launches(const AxtbBatch* b);
+void axtb_gpu_batch_destroy(AxtbBatch* b);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AXTB_GPU_H */

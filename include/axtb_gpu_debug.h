@@ -1,0 +1,37 @@
+/* axtb_gpu_debug.h - introspection of a batch after axtb_gpu_batch_run, for kernel-level
+ * parity tests. No reference counterpart: axtb's own unit tests reach the same intermediates
+ * through crate-internal functions (coordination numbers crates/axtb/src/ncoord.rs:39,
+ * AO matrices crates/axtb/src/hamiltonian.rs:77-94, density crates/axtb/src/xtb.rs:1033-1038).
+ */
+#ifndef AXTB_GPU_DEBUG_H
+#define AXTB_GPU_DEBUG_H
+
+#include "axtb_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum AxtbDebugQuantity {
+    AXTB_DBG_CN = 0,          /* nat GFN2 coordination numbers */
+    AXTB_DBG_OVERLAP = 1,     /* nao*nao overlap, column-major */
+    AXTB_DBG_H0 = 2,          /* nao*nao core Hamiltonian */
+    AXTB_DBG_DIPOLE = 3,      /* 3 planes of nao*nao dipole integrals (about the column AO's atom) */
+    AXTB_DBG_QUADRUPOLE = 4,  /* 6 planes of nao*nao traceless quadrupole integrals */
+    AXTB_DBG_DENSITY = 5,     /* nao*nao density of the last iteration */
+    AXTB_DBG_FOCK = 6,        /* nao*nao last Fock matrix */
+    AXTB_DBG_EMO = 7,         /* nao orbital energies */
+    AXTB_DBG_FOCC = 8,        /* nao occupations */
+    AXTB_DBG_WDENSITY = 9,    /* nao*nao energy-weighted density (after a gradient run) */
+    AXTB_DBG_EEQ = 10,        /* nat EEQ start charges */
+    AXTB_DBG_LINV = 11,       /* nao*nao inverse Cholesky factor of the overlap */
+};
+
+/* Copy quantity `what` of molecule `mol` of the last run into host memory `out`. */
+int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AXTB_GPU_DEBUG_H */

@@ -1,0 +1,115 @@
+"""Parity of the sm_100a engine with the CPU oracle and axtb's recorded results (GPU).
+
+Bars: |dE| <= 1e-9 Eh and max|dG| <= 1e-8 Eh/bohr against the FP64 oracle at SCF accuracy 1e-6;
+AO matrices and coordination numbers to 1e-12 absolute; axtb's recorded energies to 1e-9 Eh.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+E_TOL, G_TOL = 1e-9, 1e-8
+
+
+def _mol(golden, cid):
+    c = golden[cid]
+    return np.array(c["numbers"]), np.array(c["positions"]), c["charge"], c["uhf"]
+
+
+@pytest.mark.parametrize("cid", ["struct-water", "struct-caffeine", "struct-ferrocene", "struct-zncl4"])
+def test_integrals_match_oracle(engine, golden, cid):
+    z, x, q, u = _mol(golden, cid)
+    b = engine.Batch([(z, x, q, u)], accuracy=1e-6, max_iter=1)
+    b.run(gradient=False)
+    cn, S, H, D, Q = O.integrals(z, x, accuracy=1e-6)
+    assert np.abs(b.debug(0, "cn") - cn).max() < 1e-12
+    assert np.abs(b.debug(0, "overlap") - S).max() < 1e-12
+    assert np.abs(b.debug(0, "h0") - H).max() < 1e-12
+    assert np.abs(b.debug(0, "dipole") - D).max() < 1e-12
+    assert np.abs(b.debug(0, "quadrupole") - Q).max() < 1e-12
+
+
+@pytest.mark.parametrize("cid", ["struct-water", "struct-caffeine", "struct-ferrocene", "struct-zncl4",
+                                 "struct-cu-nh3-4", "struct-taxol"])
+def test_singlepoint_matches_oracle(engine, golden, cid):
+    z, x, q, u = _mol(golden, cid)
+    calc = engine.Calculator(z, x, charge=q, uhf=u, accuracy=1e-6)
+    r = calc.singlepoint(x, gradient=True)
+    ref = O.singlepoint(z, x, q, u, accuracy=1e-6)
+    assert r.converged
+    assert abs(r.energy - ref["energy"]) < E_TOL, (r.energy, ref["energy"])
+    assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
+    assert np.abs(r.charges - ref["qat"]).max() < 1e-7
+    assert abs(r.energy - golden[cid]["energy"]) < E_TOL
+
+
+def test_workload_molecules_match_oracle(engine):
+    from axtb_b200 import structures as S
+
+    for z, x in [S.water_cluster(32, 0, dims=(4, 4, 2)), S.alkane(12, seed=5, gauche=0.3)]:
+        r = engine.Calculator(z, x, accuracy=1e-6).singlepoint(x)
+        ref = O.singlepoint(z, x, accuracy=1e-6)
+        assert abs(r.energy - ref["energy"]) < E_TOL
+        assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
+
+
+def test_batch_equals_single_and_oracle(engine):
+    from axtb_b200 import structures as S
+
+    mols = S.mixed_batch(24, seed=11)
+    res = engine.Batch(mols, accuracy=1e-6).run(gradient=True)
+    for (z, x), r in zip(mols[:6], res[:6]):
+        ref = O.singlepoint(z, x, accuracy=1e-6)
+        assert r.status == 0
+        assert abs(r.energy - ref["energy"]) < E_TOL
+        assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
+
+
+def test_golden_energies(engine, golden):
+    ids = [c for c in golden if c.startswith("el-")][:40] + ["struct-anthracene2", "struct-tyr-xab",
+                                                             "struct-s229-cl", "struct-beni-acetone"]
+    mols = [(np.array(golden[c]["numbers"]), np.array(golden[c]["positions"]), golden[c]["charge"],
+             golden[c]["uhf"]) for c in ids]
+    res = engine.Batch(mols, accuracy=1e-6).run(gradient=False)
+    bad = [(c, r.energy - golden[c]["energy"], r.status) for c, r in zip(ids, res)
+           if r.status != 0 or abs(r.energy - golden[c]["energy"]) >= E_TOL]
+    assert not bad, bad
+
+
+def test_gradient_finite_differences(engine, golden):
+    z, x, q, u = _mol(golden, "struct-caffeine")
+    calc = engine.Calculator(z, x, accuracy=1e-8)
+    g = calc.singlepoint(x).gradient
+    h = 1e-4
+    for i, k in [(0, 0), (5, 1), (12, 2), (20, 0)]:
+        xp, xm = x.copy(), x.copy()
+        xp[i, k] += h
+        xm[i, k] -= h
+        fd = (calc.singlepoint(xp, gradient=False).energy - calc.singlepoint(xm, gradient=False).energy) / (2 * h)
+        assert abs(fd - g[i, k]) < 2e-7
+
+
+def test_deterministic(engine, golden):
+    z, x, q, u = _mol(golden, "struct-caffeine")
+    b = engine.Batch([(z, x, q, u)], accuracy=1e-6)
+    r1 = b.run()[0]
+    r2 = b.run()[0]
+    assert r1.energy == r2.energy
+    assert np.array_equal(r1.gradient, r2.gradient)
+
+
+def test_input_errors(engine):
+    from axtb_b200 import AxtbError
+
+    with pytest.raises(AxtbError) as e:
+        engine.Calculator([8, 1, 1], charge=0.5)
+    assert e.value.kind == "input"
+    calc = engine.Calculator([8, 1, 1])
+    with pytest.raises(AxtbError) as e:
+        calc.singlepoint(np.zeros((3, 3)))
+    assert e.value.kind == "input"
+    with pytest.raises(AxtbError) as e:
+        calc.singlepoint(np.full((3, 3), np.nan))
+    assert e.value.kind == "input"
