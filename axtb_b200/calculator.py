@@ -186,6 +186,16 @@ class Batch:
             raise AxtbError(rc, _lib.last_error(None))
         return st
 
+    def set_profiling(self, enable: bool = True):
+        _lib.load().axtb_gpu_batch_set_profiling(self._b, int(bool(enable)))
+
+    def profile(self) -> dict:
+        import json
+
+        buf = C.create_string_buffer(1 << 16)
+        _lib.load().axtb_gpu_batch_profile(self._b, buf, 1 << 16)
+        return json.loads(buf.value.decode())
+
     @property
     def stream(self) -> int:
         return _lib.load().axtb_gpu_batch_stream(self._b) or 0

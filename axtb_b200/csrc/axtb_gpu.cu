@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <queue>
@@ -228,12 +229,34 @@ struct AxtbBatch {
 
     void build(const vector<HostMol>& in, const Opt& o);
     void run(bool want_grad, bool warm = false);
+    // profiling and traffic accounting
+    struct Rec {
+        const char* name;
+        cudaEvent_t e0, e1;
+        double flops, bytes;
+    };
+    struct Acc {
+        long long launches = 0;
+        double ms = 0, flops = 0, bytes = 0;
+    };
+    bool profiling = false;
+    vector<Rec> recs;
+    std::map<std::string, Acc> prof;
+    int* h_act = nullptr;          // pinned copy of the active flags
+    double* h_stage = nullptr;     // pinned staging for positions and results
+    size_t h_stage_len = 0;
+    long long h2d_bytes = 0, d2h_bytes = 0;
+    void begin_launch(const char* name, double flops, double bytes);
+    void end_launch();
+    void resolve_profile();
     void extract(AxtbResult* outs, int32_t* status, bool want_grad);
     void upload_positions(const double* host_xyz, bool device_ptr);
     ~AxtbBatch();
 };
 
 AxtbBatch::~AxtbBatch() {
+    if (h_act) cudaFreeHost(h_act);
+    if (h_stage) cudaFreeHost(h_stage);
     if (dmem) cudaFree(dmem);
     if (hpin) cudaFreeHost(hpin);
     if (st) cudaStreamDestroy(st);
@@ -441,8 +464,12 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     vector<int> big, small_off(grid + 1, 0), small_list;
     {
         vector<std::pair<double, int>> smalls;
+        // molecules from this many AOs on take the whole grid (AXTB_TEAM_BIG_NAO overrides, e.g.
+        // to run small molecules through the grid-wide path in tests)
+        int big_nao = 1024;
+        if (const char* e = std::getenv("AXTB_TEAM_BIG_NAO")) big_nao = std::max(1, std::atoi(e));
         for (int m = 0; m < nmol; m++) {
-            if (m_nao[m] >= 1024) big.push_back(m);
+            if (m_nao[m] >= big_nao) big.push_back(m);
             else smalls.push_back({std::pow((double)m_nao[m] + 32.0, 3.0), m});
         }
         std::sort(smalls.begin(), smalls.end(), [](auto& x, auto& y) { return x.first > y.first; });
@@ -687,6 +714,9 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     d_eatm = ar.take<double>(nmol);
     e_rep.assign(nmol, 0.0);
     e_atm.assign(nmol, 0.0);
+    CK(cudaMallocHost(&h_act, sizeof(int) * nmol));
+    h_stage_len = std::max<size_t>((size_t)natT * 12 + (size_t)nshT + (size_t)nmol * 16, 1024);
+    CK(cudaMallocHost(&h_stage, sizeof(double) * h_stage_len));
     CK(cudaStreamSynchronize(st));
 }
 
@@ -763,17 +793,91 @@ inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) /
 
 }  // namespace
 
+// positions of every molecule into HBM: from a device pointer directly, from host memory
+// through the pinned staging buffer
 void AxtbBatch::upload_positions(const double* x, bool device_ptr) {
-    CK(cudaMemcpyAsync(S.xyz, x, sizeof(double) * 3 * natT, device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                       st));
+    size_t bytes = sizeof(double) * 3 * natT;
+    if (device_ptr) {
+        CK(cudaMemcpyAsync(S.xyz, x, bytes, cudaMemcpyDeviceToDevice, st));
+        return;
+    }
+    std::memcpy(h_stage, x, bytes);
+    CK(cudaMemcpyAsync(S.xyz, h_stage, bytes, cudaMemcpyHostToDevice, st));
+    h2d_bytes += (long long)bytes;
+}
+
+// Optional per-launch timing: CUDA events recorded on the batch stream around each kernel,
+// resolved after the run; with the algorithmic work of each launch (FLOPs of the dense algebra,
+// bytes of the matrix passes) for the roofline report.
+void AxtbBatch::begin_launch(const char* name, double flops, double bytes) {
+    launches++;
+    if (!profiling) return;
+    Rec r;
+    r.name = name;
+    r.flops = flops;
+    r.bytes = bytes;
+    CK(cudaEventCreate(&r.e0));
+    CK(cudaEventCreate(&r.e1));
+    CK(cudaEventRecord(r.e0, st));
+    recs.push_back(r);
+}
+
+void AxtbBatch::end_launch() {
+    if (!profiling) return;
+    CK(cudaEventRecord(recs.back().e1, st));
+}
+
+void AxtbBatch::resolve_profile() {
+    if (!profiling) return;
+    CK(cudaStreamSynchronize(st));
+    for (auto& r : recs) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+        auto& a = prof[r.name];
+        a.launches += 1;
+        a.ms += ms;
+        a.flops += r.flops;
+        a.bytes += r.bytes;
+        cudaEventDestroy(r.e0);
+        cudaEventDestroy(r.e1);
+    }
+    recs.clear();
 }
 
 void AxtbBatch::run(bool want_grad, bool warm) {
     using namespace axg;
     launches = 0;
-    auto L = [&](void) { launches++; };
     const int T = 256;
     long long nn = nnT;
+#define LAUNCH(name, flops, bytes, ...)  \
+    do {                                 \
+        begin_launch(name, flops, bytes); \
+        __VA_ARGS__;                     \
+        end_launch();                    \
+    } while (0)
+    // algorithmic work of the matrix passes over the molecules in `act` (1 = included)
+    auto mat_bytes = [&](const vector<int>& act, double per_n2) {
+        double s = 0.0;
+        for (int m = 0; m < nmol; m++)
+            if (act[m]) s += per_n2 * 8.0 * (double)mols[m].nao * mols[m].nao;
+        return s;
+    };
+    auto eig_flops = [&](const vector<int>& act) {
+        double s = 0.0;
+        for (int m = 0; m < nmol; m++)
+            if (act[m]) {
+                double n = mols[m].nao, k = std::ceil(mols[m].nalpha);
+                s += 4.0 * n * n * n + 4.0 / 3.0 * n * n * n + 6.0 * n * n * k;
+            }
+        return s;
+    };
+    auto w_flops = [&](const vector<int>& act) {
+        double s = 0.0;
+        for (int m = 0; m < nmol; m++)
+            if (act[m]) s += 2.0 * mols[m].nao * mols[m].nao * std::ceil(mols[m].nalpha);
+        return s;
+    };
+    vector<int> all(nmol, 1), act(nmol, 1);
     // reset per-run state
     CK(cudaMemsetAsync(S.status, 0, sizeof(int) * nmol, st));
     CK(cudaMemsetAsync(S.S, 0, sizeof(double) * nn * 11, st));  // S, H0, D(3), Q(6) contiguous
@@ -784,94 +888,72 @@ void AxtbBatch::run(bool want_grad, bool warm) {
     CK(cudaMemsetAsync(S.terms, 0, sizeof(double) * nmol * 8, st));
     CK(cudaMemsetAsync(S.ts, 0, sizeof(double) * nmol, st));
     // geometry
-    k_cn<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-    L();
-    k_selfenergy<<<blocks_for(std::max(natT, nshT), T), T, 0, st>>>(B, S);
-    L();
-    k_repulsion<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-    L();
-    double* e_tmp = S.energy;  // per-molecule scratch for the fixed energies
-    k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, S.e_fixed);
-    L();
+    LAUNCH("cn", 0, 0, k_cn<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+    LAUNCH("selfenergy", 0, 0, k_selfenergy<<<blocks_for(std::max(natT, nshT), T), T, 0, st>>>(B, S));
+    LAUNCH("repulsion", 0, 0, k_repulsion<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+    LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, S.e_fixed));
     CK(cudaMemsetAsync(S.e_atom, 0, sizeof(double) * natT, st));
     // D4 three-body at q = 0 with dgw/dCN weights
     CK(cudaMemsetAsync(P.eeq_q, 0, sizeof(double) * natT, st));
-    k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1);
-    L();
-    k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT);
-    L();
-    k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0);
-    L();
-    k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm);
-    L();
-    (void)e_tmp;
+    LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1));
+    LAUNCH("atm_tables", 0, 0, k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT));
+    LAUNCH("atm", 0, 0, k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0));
+    LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm));
     // integrals
-    k_integrals<<<blocks_for(npdT, 128), 128, 0, st>>>(B, S, d_pd0, npdT);
-    L();
+    LAUNCH("integrals", 0, mat_bytes(all, 11.0), k_integrals<<<blocks_for(npdT, 128), 128, 0, st>>>(B, S, d_pd0, npdT));
     // overlap factorisation and EEQ start
     void* args[] = {&B, &S, &P, nullptr};
     int ph = PH_OVERLAP;
     args[3] = &ph;
-    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
-    L();
+    double chol_flops = 0.0;
+    for (int m = 0; m < nmol; m++) chol_flops += (1.0 / 3.0 + 2.0 / 3.0) * std::pow((double)mols[m].nao, 3.0);
+    LAUNCH("team_overlap", chol_flops, 0,
+           CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     bool eeq = opt.guess == 0 && !warm;
     if (warm) {
-        k_start_warm<<<nmol, T, 0, st>>>(B, S);
-        L();
+        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S));
     } else if (eeq) {
-        k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT);
-        L();
+        LAUNCH("eeq_matrix", 0, 0, k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT));
         ph = PH_EEQ;
-        CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
-        L();
+        double f = 0.0;
+        for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
+        LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     }
-    if (!warm) {
-        k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0);
-        L();
-    }
+    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0));
     // SCF
-    vector<int> act(nmol);
     for (int it = 1; it <= opt.max_iter; it++) {
-        k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0);
-        L();
-        k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-        L();
-        k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles);
-        L();
+        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0));
+        LAUNCH("potentials", 0, 0, k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+        LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
         ph = PH_EIGEN;
-        CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
-        L();
-        k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S);
-        L();
-        k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S);
-        L();
-        k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2);
-        L();
-        k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-        L();
-        k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap);
-        L();
-        CK(cudaMemcpyAsync(act.data(), S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+        LAUNCH("team_eigen", eig_flops(act), 0,
+               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+        LAUNCH("mulliken", 0, mat_bytes(act, 12.0),
+               k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S));
+        LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
+        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2));
+        LAUNCH("energy", 0, 0, k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+        LAUNCH("broyden", 0, 0, k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap));
+        CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+        std::copy(h_act, h_act + nmol, act.begin());
         if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
     }
-    if (!want_grad) return;
-    ph = PH_WDENS;
-    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st));
-    L();
-    if (npairT > 0) {
-        k_h0_gradient<<<blocks_for(npairT, 128), 128, 0, st>>>(B, S, d_pair0, npairT, S.pair_buf);
-        L();
+    if (want_grad) {
+        ph = PH_WDENS;
+        LAUNCH("team_wdens", w_flops(all), 0,
+               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+        if (npairT > 0)
+            LAUNCH("h0_gradient", 0, mat_bytes(all, 2.0),
+                   k_h0_gradient<<<blocks_for(npairT, 128), 128, 0, st>>>(B, S, d_pair0, npairT, S.pair_buf));
+        LAUNCH("h0_gather", 0, 0, k_h0_gather<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_pair0, S.pair_buf));
+        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 1));
+        LAUNCH("grad_pairs", 0, 0, k_grad_pairs<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+        LAUNCH("cn_chain", 0, 0, k_cn_chain<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
     }
-    k_h0_gather<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_pair0, S.pair_buf);
-    L();
-    k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 1);
-    L();
-    k_grad_pairs<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-    L();
-    k_cn_chain<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S);
-    L();
+#undef LAUNCH
     CK(cudaGetLastError());
+    resolve_profile();
 }
 
 #include "../../include/axtb_gpu_debug.h"

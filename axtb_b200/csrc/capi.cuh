@@ -35,6 +35,8 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     CK(cudaMemcpyAsync(qsh.data(), S.qsh_out, sizeof(double) * nshT, cudaMemcpyDeviceToHost, st));
     if (want_grad) CK(cudaMemcpyAsync(grad.data(), S.grad, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    d2h_bytes += (long long)(sizeof(double) * (nmol * 14 + (size_t)natT * 10 + nshT) + sizeof(int) * nmol * 3) +
+                 (want_grad ? (long long)sizeof(double) * natT * 3 : 0);
     for (int m = 0; m < nmol; m++) {
         AxtbResult& r = outs[m];
         int a0 = m_at0[m], nat = mols[m].nat;
@@ -299,6 +301,38 @@ int axtb_gpu_batch(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, i
 }
 
 // ---- introspection (include/axtb_gpu_debug.h)
+int axtb_gpu_batch_set_profiling(AxtbBatch* b, int32_t enable) {
+    if (!b) return AXTB_ERR_INPUT;
+    b->profiling = enable != 0;
+    b->prof.clear();
+    b->h2d_bytes = b->d2h_bytes = 0;
+    return AXTB_OK;
+}
+
+int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
+    if (!b) return AXTB_ERR_INPUT;
+    std::string s = "{\"kernels\": {";
+    bool first = true;
+    for (auto& kv : b->prof) {
+        char tmp[256];
+        std::snprintf(tmp, sizeof tmp, "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"flops\": %.6e, \"bytes\": %.6e}",
+                      first ? "" : ", ", kv.first.c_str(), kv.second.launches, kv.second.ms, kv.second.flops,
+                      kv.second.bytes);
+        s += tmp;
+        first = false;
+    }
+    char tail[160];
+    std::snprintf(tail, sizeof tail, "}, \"h2d_bytes\": %lld, \"d2h_bytes\": %lld, \"grid\": %d}", b->h2d_bytes,
+                  b->d2h_bytes, b->grid);
+    s += tail;
+    if (buf && len > 0) {
+        size_t n = std::min(len - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return (int)s.size();
+}
+
 int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out) {
     if (!b || !out || mol < 0 || mol >= b->nmol) return AXTB_ERR_INPUT;
     return guarded(&b->err, [&] {

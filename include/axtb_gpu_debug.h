@@ -27,6 +27,13 @@ enum AxtbDebugQuantity {
     AXTB_DBG_LINV = 11,       /* nao*nao inverse Cholesky factor of the overlap */
 };
 
+/* Per-kernel timing: with profiling on, every kernel launch of a run is bracketed by CUDA
+ * events on the batch's stream; axtb_gpu_batch_profile writes a JSON object with, per kernel,
+ * launches, milliseconds, algorithmic FLOPs and bytes, plus the host<->device bytes of the
+ * public-API runs. Enabling resets the counters. Returns the JSON length. */
+int axtb_gpu_batch_set_profiling(AxtbBatch* b, int32_t enable);
+int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len);
+
 /* Copy quantity `what` of molecule `mol` of the last run into host memory `out`. */
 int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out);
 
