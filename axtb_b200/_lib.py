@@ -59,6 +59,8 @@ SIGNATURES = {
     "axtb_gpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "axtb_gpu_batch_launches": (C.c_int64, [C.c_void_p]),
     "axtb_gpu_batch_destroy": (None, [C.c_void_p]),
+    "axtb_gpu_density_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "axtb_gpu_batch_debug": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, PD]),
     "axtb_gpu_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "axtb_gpu_batch_profile": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),

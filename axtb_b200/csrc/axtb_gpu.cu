@@ -956,5 +956,135 @@ void AxtbBatch::run(bool want_grad, bool warm) {
     resolve_profile();
 }
 
+// ------------------------------------------------------------------ allocation-free density
+// Eigenvalues, Fermi occupations and density of one molecule from its Fock and overlap
+// matrices (the team kernel's overlap and eigen phases on one CTA) with every scratch buffer in
+// one file-scope device array instead of memory from cudaMalloc: for callers that cannot
+// allocate device memory themselves (code running inside another framework's stream-ordered
+// memory pool or under a fixed device-memory budget, where a cudaMalloc would fail or would
+// synchronise the device and stall unrelated work). The array exists once per device for as
+// long as the library is loaded; it bounds the molecule to STATIC_MAX_NAO basis functions.
+namespace {
+constexpr int STATIC_MAX_NAO = 256;
+constexpr long long STATIC_PLANE = (long long)STATIC_MAX_NAO * STATIC_MAX_NAO;  // doubles per matrix
+constexpr long long STATIC_WK = 274LL * STATIC_MAX_NAO + 8192 + 64;             // team workspace
+constexpr long long STATIC_VEC = 8LL * STATIC_MAX_NAO;                           // d, e, tau + spare
+constexpr long long STATIC_PIV = STATIC_PLANE / 8;                               // pivot bytes, as doubles
+constexpr long long STATIC_PAR = 64;                                             // small parameters
+constexpr long long STATIC_DOUBLES = 7 * STATIC_PLANE + STATIC_WK + STATIC_VEC + STATIC_PIV + STATIC_PAR;
+static __device__ __align__(256) double g_density_scratch[STATIC_DOUBLES];  // 4.25 MiB
+
+std::mutex g_static_mu;
+double* g_static_addr[256] = {nullptr};
+}  // namespace
+
+namespace axg {
+// one CTA: parameters into the static area, then the factorisation and the eigen phase
+__global__ void __launch_bounds__(TEAM_THREADS)
+    k_density_static(Batch B, State S, TeamPlan P, int nao, double nalpha, double nbeta, int* d_status) {
+    if (threadIdx.x == 0) {
+        *const_cast<int*>(B.m_nao) = nao;
+        *const_cast<int*>(B.m_ao0) = 0;
+        *const_cast<long long*>(B.m_mat0) = 0;
+        *const_cast<long long*>(P.m_wk0) = 0;
+        *const_cast<double*>(B.m_nalpha) = nalpha;
+        *const_cast<double*>(B.m_nbeta) = nbeta;
+        S.status[0] = 0;  // the array keeps the previous call's words
+        S.kocc[0] = 0;
+    }
+    __syncthreads();
+    Team one{0, 1, false};
+    mol_overlap(one, B, S, P, 0);
+    mol_eigen(one, B, S, P, 0);
+    if (threadIdx.x == 0 && d_status) *d_status = S.status[0];
+}
+}  // namespace axg
+
+extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_overlap, int32_t nao, double nalpha,
+                                       double nbeta, double kt, double* d_emo, double* d_focc, double* d_density,
+                                       int32_t* d_status, void* stream) {
+    if (!d_fock || !d_overlap || !d_emo || !d_focc || !d_density) {
+        g_last_error = "axtb_gpu_density_static: null pointer argument";
+        return AXTB_ERR_INPUT;
+    }
+    if (nao <= 0 || nao > STATIC_MAX_NAO) {
+        g_last_error = "axtb_gpu_density_static: nao must be in 1.." + std::to_string(STATIC_MAX_NAO) + ", got " +
+                       std::to_string(nao);
+        return AXTB_ERR_INPUT;
+    }
+    if (!(nalpha >= 0.0 && nbeta >= 0.0 && nalpha <= nao && nbeta <= nao) || !(kt >= 0.0)) {
+        g_last_error = "axtb_gpu_density_static: electron counts must be in [0, nao] and kT >= 0";
+        return AXTB_ERR_INPUT;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) {
+        g_last_error = "axtb_gpu_density_static: no current CUDA device";
+        return AXTB_ERR_DEVICE;
+    }
+    double* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_addr[dev]) {
+            // host code only holds a stand-in for the array: its device address comes from the
+            // runtime, once per device, with that device current
+            cudaError_t e = cudaGetSymbolAddress((void**)&g_static_addr[dev], g_density_scratch);
+            if (e != cudaSuccess) {
+                g_static_addr[dev] = nullptr;
+                g_last_error = std::string("axtb_gpu_density_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                return AXTB_ERR_DEVICE;
+            }
+        }
+        base = g_static_addr[dev];
+    }
+    double* p = base;
+    auto take = [&](long long n) {
+        double* r = p;
+        p += n;
+        return r;
+    };
+    axg::Batch B{};
+    axg::State S{};
+    axg::TeamPlan P{};
+    S.scr1 = take(STATIC_PLANE);
+    S.Linv = take(STATIC_PLANE);
+    S.Fp = take(STATIC_PLANE);
+    S.Z = take(STATIC_PLANE);
+    S.C = take(STATIC_PLANE);
+    S.scr2 = take(STATIC_PLANE);
+    S.scr3 = take(STATIC_PLANE);
+    P.wk = take(STATIC_WK);
+    double* vec = take(STATIC_VEC);
+    S.dtri = vec;
+    S.etri = vec + STATIC_MAX_NAO;
+    S.tau = vec + 2 * STATIC_MAX_NAO;
+    S.piv = reinterpret_cast<unsigned char*>(take(STATIC_PIV));
+    double* par = take(STATIC_PAR);
+    B.m_nao = reinterpret_cast<const int*>(par + 0);
+    B.m_ao0 = reinterpret_cast<const int*>(par + 1);
+    B.m_mat0 = reinterpret_cast<const long long*>(par + 2);
+    P.m_wk0 = reinterpret_cast<const long long*>(par + 3);
+    B.m_nalpha = par + 4;
+    B.m_nbeta = par + 5;
+    S.ts = par + 6;
+    S.kocc = reinterpret_cast<int*>(par + 7);
+    S.status = reinterpret_cast<int*>(par + 8);
+    S.red = par + 16;
+    S.S = const_cast<double*>(d_overlap);
+    S.F = const_cast<double*>(d_fock);
+    S.emo = d_emo;
+    S.focc = d_focc;
+    S.P = d_density;
+    B.nmol = 1;
+    B.kt = kt;
+    P.max_chunks = 16;
+    axg::k_density_static<<<1, axg::TEAM_THREADS, 0, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta, d_status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_error = std::string("axtb_gpu_density_static: launch: ") + cudaGetErrorString(e);
+        return AXTB_ERR_DEVICE;
+    }
+    return AXTB_OK;
+}
+
 #include "../../include/axtb_gpu_debug.h"
 #include "capi.cuh"

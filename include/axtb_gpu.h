@@ -129,6 +129,25 @@ void* axtb_gpu_batch_stream(AxtbBatch* b);
 int64_t axtb_gpu_batch_launches(const AxtbBatch* b);
 void axtb_gpu_batch_destroy(AxtbBatch* b);
 
+/* Orbital energies, Fermi occupations and density matrix of one molecule from its Fock matrix
+ * and overlap matrix (FC = SCe with Fermi smearing at kT for nalpha + nbeta electrons), without
+ * allocating any device memory. No counterpart in the reference: it is for callers that cannot
+ * call cudaMalloc, e.g. code inside another framework's stream-ordered memory pool or under a
+ * fixed device-memory budget, where an allocation would fail or would synchronise the device.
+ * All scratch lives in one array in the library's device image: 4.25 MiB, held by every GPU
+ * that loads the library until the process exits, which limits nao to 256.
+ * Inputs d_fock and d_overlap (nao*nao, column-major) and outputs d_emo, d_focc (nao) and
+ * d_density (nao*nao) are device pointers the caller allocates; d_status (optional, device)
+ * receives the molecule's status bits (0 = ok). The work is queued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream) and the call returns without waiting.
+ * The first call on a device looks the array's device address up; make that first call before
+ * any stream capture. Calls share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be ordered by the caller. Returns AXTB_ERR_INPUT for nao
+ * outside 1..256 or bad arguments, AXTB_ERR_DEVICE when the launch fails. */
+int axtb_gpu_density_static(const double* d_fock, const double* d_overlap, int32_t nao, double nalpha, double nbeta,
+                            double kt, double* d_emo, double* d_focc, double* d_density, int32_t* d_status,
+                            void* stream);
+
 #ifdef __cplusplus
 }
 #endif
