@@ -515,7 +515,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addD((size_t)nvecT * 4 + (size_t)nhist * 2 + (size_t)nmol * hist_cap * hist_cap * 2 + (size_t)nmol * hist_cap);
     addD((size_t)nmol * 14);
     addD((size_t)natT * 5 + (size_t)std::max(npairT, 1LL) * 5 + natT + natT * 5);
-    addD((size_t)grid * 8 + 64);
+    addD((size_t)grid * 64 + 64);
     addD((size_t)nsqT * 3 + natT * 2);
     addD((size_t)nwk);
     addL(nmol * 5);
@@ -695,7 +695,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.pair_buf = ar.take<double>((size_t)std::max(npairT, 1LL) * 5);
     s.e_atom = ar.take<double>(natT);
     s.e_terms = ar.take<double>(natT * 5);
-    s.red = ar.take<double>((size_t)grid * 8 + 64);
+    s.red = ar.take<double>((size_t)grid * 64 + 64);  // team partials: 64 per CTA
     s.eeq_A = ar.take<double>((size_t)nsqT * 3);
     // team plan
     P.big = upI(big);

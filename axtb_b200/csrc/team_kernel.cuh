@@ -105,7 +105,11 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* vbuf = wk;
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
-    team_tridiag(t, Fp, n, n, d, e, tau, vbuf, pbuf, ppart, S.red, P.max_chunks);
+    {
+        double* Vp = wk + 2 * n + (long long)P.max_chunks * n;  // the back-transform's vb area (64 n)
+        team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
+                             P.max_chunks);
+    }
     double* emo = S.emo + ao0;
     team_bisect(t, d, e, n, emo, wk);
     // Fermi filling of both spins (warp 0 of CTA 0), kocc and -TS

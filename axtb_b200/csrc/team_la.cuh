@@ -284,6 +284,178 @@ __device__ void team_tridiag(const Team& t, double* A, long long lda, int n, dou
     t.sync();
 }
 
+// ---------------------------------------------------------------------------------- blocked
+// The same reduction in panels of NBP columns (the LAPACK dsytrd/dlatrd scheme): within a
+// panel, column j is first brought up to date with the panel's earlier reflectors, its
+// Householder vector is formed, and w = tau (A v - W (V^T v) - V (W^T v)) uses the trailing matrix
+// as it was at the start of the panel (one read-only pass, no writes); after the panel the
+// trailing matrix takes the rank-2*NBP update A -= V W^T + W V^T on GEMMs. V and W are n x NBP
+// (leading dimension n); the reflectors end up in A exactly as in team_tridiag.
+constexpr int NBP = 32;
+
+// ys[q] = V[r0:n, q] . v (q < c) and ys[c + q] = W[r0:n, q] . v, into shared memory
+__device__ void team_panel_dots(const Team& t, const double* V, const double* W, long long ldv, const double* v, int r0,
+                                int n, int c, double* ys, double* gpart) {
+    __syncthreads();
+    int nq = 2 * c;
+    int m = n - r0, per = (m + t.size - 1) / t.size;
+    int rb0 = r0 + t.rank * per, rb1 = min(n, rb0 + per);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int q = wid; q < nq; q += nw) {
+        const double* X = q < c ? V + (long long)q * ldv : W + (long long)(q - c) * ldv;
+        double s = 0.0;
+        for (int i = rb0 + lane; i < rb1; i += 32) s = fma(X[i], v[i], s);
+        s = warp_sum(s);
+        if (lane == 0) {
+            if (t.global) gpart[t.rank * 64 + q] = s;
+            else ys[q] = s;
+        }
+    }
+    if (t.global) {
+        t.sync();
+        if ((int)threadIdx.x < nq) {
+            double s = 0.0;
+            for (int r = 0; r < t.size; r++) s += gpart[r * 64 + threadIdx.x];
+            ys[threadIdx.x] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// partial sums of A[r0:n, r0:n] v over column chunks: warps own 64-row tiles (two rows per lane)
+// x column chunks, four columns per step with independent accumulators; ppart[ch * n + row]
+__device__ int team_symv_partials(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
+                                  double* ppart, int max_chunks) {
+    int m = n - r0;
+    int rt = (m + 63) / 64;
+    int nch = max(1, min(max_chunks, (t.nwarps() * 2 + rt - 1) / rt));
+    int cw = (m + nch - 1) / nch;
+    int lane = threadIdx.x & 31;
+    for (int it = t.warp(); it < rt * nch; it += t.nwarps()) {
+        int tr = it % rt, ch = it / rt;
+        int ra = r0 + tr * 64 + lane, rb = ra + 32;
+        bool oka = ra < n, okb = rb < n;
+        int la = oka ? ra : n - 1, lb = okb ? rb : n - 1;
+        int c0 = r0 + ch * cw, c1 = min(n, c0 + cw);
+        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+        int c = c0;
+        for (; c + 3 < c1; c += 4) {
+            const double* p0 = A + (long long)c * lda;
+            double x0 = p0[la], x1 = p0[lda + la], x2 = p0[2 * lda + la], x3 = p0[3 * lda + la];
+            double y0 = p0[lb], y1 = p0[lda + lb], y2 = p0[2 * lda + lb], y3 = p0[3 * lda + lb];
+            double v0 = v[c], v1 = v[c + 1], v2 = v[c + 2], v3 = v[c + 3];
+            a0 = fma(x0, v0, a0);
+            a1 = fma(x1, v1, a1);
+            a0 = fma(x2, v2, a0);
+            a1 = fma(x3, v3, a1);
+            b0 = fma(y0, v0, b0);
+            b1 = fma(y1, v1, b1);
+            b0 = fma(y2, v2, b0);
+            b1 = fma(y3, v3, b1);
+        }
+        for (; c < c1; c++) {
+            double vc = v[c];
+            a0 = fma(A[la + (long long)c * lda], vc, a0);
+            b0 = fma(A[lb + (long long)c * lda], vc, b0);
+        }
+        if (oka) ppart[(long long)ch * n + ra] = a0 + a1;
+        if (okb) ppart[(long long)ch * n + rb] = b0 + b1;
+    }
+    return nch;
+}
+
+__device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
+                                     double* V, double* W, double* vbuf, double* pbuf, double* ppart, double* gred,
+                                     int max_chunks) {
+    __shared__ double ys[64];
+    const long long ldv = n;
+    int nrefl = n - 2;
+    for (int j0 = 0; j0 < nrefl; j0 += NBP) {
+        int nb = min(NBP, nrefl - j0);
+        for (int c = 0; c < nb; c++) {
+            int j = j0 + c, r0 = j + 1;
+            // (1) column j brought up to date with the panel's earlier reflectors
+            if (c > 0) {
+                for (int i = j + t.tid(); i < n; i += t.nthreads()) {
+                    double s = 0.0;
+                    for (int q = 0; q < c; q++)
+                        s += V[i + q * ldv] * W[j + q * ldv] + W[i + q * ldv] * V[j + q * ldv];
+                    A[i + (long long)j * lda] -= s;
+                }
+                t.sync();
+            }
+            // (2) Householder vector of A[r0:n, j]
+            double alpha = A[r0 + (long long)j * lda];
+            double xs = 0.0;
+            for (int i = r0 + 1 + t.tid(); i < n; i += t.nthreads()) xs += sq(A[i + (long long)j * lda]);
+            double xnorm2 = team_sum(t, xs, gred);
+            double beta, tj, scale;
+            if (xnorm2 == 0.0) {
+                tj = 0.0;
+                beta = alpha;
+                scale = 0.0;
+            } else {
+                beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+                tj = (beta - alpha) / beta;
+                scale = 1.0 / (alpha - beta);
+            }
+            for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
+                double v = i == r0 ? 1.0 : A[i + (long long)j * lda] * scale;
+                vbuf[i] = v;
+                V[i + c * ldv] = v;
+                if (i > r0) A[i + (long long)j * lda] = v;
+            }
+            if (t.tid() == 0) {
+                e[j] = beta;
+                tau[j] = tj;
+                d[j] = A[j + (long long)j * lda];
+                A[r0 + (long long)j * lda] = beta;
+            }
+            t.sync();
+            // (3) w = tau (A v - W V^T v - V W^T v) - tau^2/2 (..) v
+            if (tj != 0.0) {
+                int nch = team_symv_partials(t, A, lda, r0, n, vbuf, ppart, max_chunks);
+                team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);
+                t.sync();
+                double pv = 0.0;
+                for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
+                    double s = 0.0;
+                    for (int ch = 0; ch < nch; ch++) s += ppart[(long long)ch * n + i];
+                    for (int q = 0; q < c; q++) s -= W[i + q * ldv] * ys[q] + V[i + q * ldv] * ys[c + q];
+                    s *= tj;
+                    pbuf[i] = s;
+                    pv += s * vbuf[i];
+                }
+                double dot = team_sum(t, pv, gred);
+                double K = -0.5 * tj * dot;
+                for (int i = r0 + t.tid(); i < n; i += t.nthreads()) W[i + c * ldv] = pbuf[i] + K * vbuf[i];
+            } else {
+                for (int i = r0 + t.tid(); i < n; i += t.nthreads()) W[i + c * ldv] = 0.0;
+            }
+            t.sync();
+        }
+        // (4) trailing update of rows and columns q0..n-1
+        int q0 = j0 + nb, mm = n - q0;
+        if (mm > 0) {
+            team_gemm(t, false, true, mm, mm, nb, -1.0, V + q0, ldv, W + q0, ldv, 1.0, A + q0 + (long long)q0 * lda, lda);
+            t.sync();
+            team_gemm(t, false, true, mm, mm, nb, -1.0, W + q0, ldv, V + q0, ldv, 1.0, A + q0 + (long long)q0 * lda, lda);
+            t.sync();
+        }
+    }
+    if (t.tid() == 0) {
+        if (n >= 2) {
+            d[n - 2] = A[(n - 2) + (long long)(n - 2) * lda];
+            e[n - 2] = A[(n - 1) + (long long)(n - 2) * lda];
+            tau[n - 2] = 0.0;
+        }
+        d[n - 1] = A[(n - 1) + (long long)(n - 1) * lda];
+        e[n - 1] = 0.0;
+        tau[n - 1] = 0.0;
+    }
+    t.sync();
+}
+
 // number of eigenvalues of the symmetric tridiagonal (d, e) below x (Sturm sequence)
 __device__ __forceinline__ int sturm_count(const double* d, const double* e, int n, double x, double pivmin) {
     int cnt = 0;
