@@ -240,6 +240,7 @@ struct AxtbBatch {
         double ms = 0, flops = 0, bytes = 0;
     };
     bool profiling = false;
+    double team_cycles[16] = {0};
     vector<Rec> recs;
     std::map<std::string, Acc> prof;
     int* h_act = nullptr;          // pinned copy of the active flags
@@ -830,6 +831,9 @@ void AxtbBatch::end_launch() {
 void AxtbBatch::resolve_profile() {
     if (!profiling) return;
     CK(cudaStreamSynchronize(st));
+    unsigned long long cyc[16];
+    CK(cudaMemcpyFromSymbol(cyc, axg::g_team_cycles, sizeof cyc));
+    for (int k = 0; k < 16; k++) team_cycles[k] += (double)cyc[k];
     for (auto& r : recs) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
@@ -847,6 +851,11 @@ void AxtbBatch::resolve_profile() {
 void AxtbBatch::run(bool want_grad, bool warm) {
     using namespace axg;
     launches = 0;
+    P.cycles = profiling ? 1 : 0;
+    if (profiling) {
+        unsigned long long z[16] = {0};
+        CK(cudaMemcpyToSymbolAsync(g_team_cycles, z, sizeof z, 0, cudaMemcpyHostToDevice, st));
+    }
     const int T = 256;
     long long nn = nnT;
 #define LAUNCH(name, flops, bytes, ...)  \

@@ -305,6 +305,7 @@ int axtb_gpu_batch_set_profiling(AxtbBatch* b, int32_t enable) {
     if (!b) return AXTB_ERR_INPUT;
     b->profiling = enable != 0;
     b->prof.clear();
+    for (double& c : b->team_cycles) c = 0.0;
     b->h2d_bytes = b->d2h_bytes = 0;
     return AXTB_OK;
 }
@@ -320,6 +321,17 @@ int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
                       kv.second.bytes);
         s += tmp;
         first = false;
+    }
+    // SM-cycle shares of the eigen phase's parts (one-CTA teams)
+    static const char* PH[8] = {"transform", "tridiagonal", "bisection", "fermi", "inverse_iteration",
+                                "back_transform", "c_matrix", "density"};
+    double tc = 0.0;
+    for (int k = 0; k < 8; k++) tc += b->team_cycles[k];
+    s += "}, \"team_eigen_phases\": {";
+    for (int k = 0; k < 8; k++) {
+        char tmp[96];
+        std::snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", k ? ", " : "", PH[k], tc > 0 ? b->team_cycles[k] / tc : 0.0);
+        s += tmp;
     }
     char tail[160];
     std::snprintf(tail, sizeof tail, "}, \"h2d_bytes\": %lld, \"d2h_bytes\": %lld, \"grid\": %d}", b->h2d_bytes,

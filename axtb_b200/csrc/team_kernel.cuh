@@ -27,7 +27,19 @@ struct TeamPlan {
     double* eeq_q;            // natT: EEQ charges
     long long eeq_plane;      // size of one EEQ plane (sum nat^2)
     int max_chunks;
+    int cycles;               // 1: accumulate per-phase SM cycles of mol_eigen into g_team_cycles
 };
+
+// per-phase cycle counters of the eigen phase (instrumentation, read by the profiler)
+__device__ unsigned long long g_team_cycles[16];
+#define TEAM_PHASE(k)                                                  \
+    do {                                                               \
+        if (P.cycles && t.tid() == 0) {                                \
+            long long now__ = clock64();                               \
+            atomicAdd(&g_team_cycles[k], (unsigned long long)(now__ - t0__)); \
+            t0__ = now__;                                              \
+        }                                                              \
+    } while (0)
 
 __device__ void mol_overlap(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
     int n = B.m_nao[m];
@@ -85,20 +97,16 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* Linv = S.Linv + mat;
     double* X = S.scr1 + mat;
     double* Fp = S.Fp + mat;
+    long long t0__ = clock64();
     // F' = L^-1 F L^-T, symmetrised
-    team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n);
+    // (L^-1 is lower triangular; F' is symmetric: its lower tiles are computed and mirrored)
+    team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n, GEMM_A_LOWER);
     t.sync();
-    team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n);
+    team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n, GEMM_B_UPPER | GEMM_LOWER_TILES);
     t.sync();
-    for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) {
-        int i = (int)(e % n), c = (int)(e / n);
-        if (i > c) {
-            double v = 0.5 * (Fp[i + (long long)c * n] + Fp[c + (long long)i * n]);
-            Fp[i + (long long)c * n] = v;
-            Fp[c + (long long)i * n] = v;
-        }
-    }
+    team_mirror_lower(t, Fp, n, 0, n);
     t.sync();
+    TEAM_PHASE(0);
     double* d = S.dtri + ao0;
     double* e = S.etri + ao0;
     double* tau = S.tau + ao0;
@@ -110,8 +118,10 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
         team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
                              P.max_chunks);
     }
+    TEAM_PHASE(1);
     double* emo = S.emo + ao0;
     team_bisect(t, d, e, n, emo, wk);
+    TEAM_PHASE(2);
     // Fermi filling of both spins (warp 0 of CTA 0), kocc and -TS
     double* focc = S.focc + ao0;
     double* occb = wk + 8;  // n entries
@@ -142,9 +152,11 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
         }
     }
     t.sync();
+    TEAM_PHASE(3);
     int k = S.kocc[m];
     double* Zm = S.Z + mat;
     team_invit(t, d, e, emo, n, k, Zm, n, S.scr1 + mat, S.scr2 + mat, S.scr3 + mat, S.piv + mat, S.P + mat, &S.status[m]);
+    TEAM_PHASE(4);
     // back-transform: vb (n x 64), tb, gm (64 x 64), y, y2 (64 x k)
     double* vb = wk + 2 * n + (long long)P.max_chunks * n;
     double* tb = vb + 64LL * n;
@@ -152,15 +164,20 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* y = gm + 64 * 64;
     double* y2 = y + 64LL * n;
     team_backtransform(t, Fp, n, tau, n, k, Zm, n, vb, tb, gm, y, y2);
+    TEAM_PHASE(5);
     // C = L^-T Z'; P = (C f) C^T
     double* Cm = S.C + mat;
-    team_gemm(t, true, false, n, k, n, 1.0, Linv, n, Zm, n, 0.0, Cm, n);
+    team_gemm(t, true, false, n, k, n, 1.0, Linv, n, Zm, n, 0.0, Cm, n, GEMM_A_UPPER);
     t.sync();
+    TEAM_PHASE(6);
     double* Cf = S.scr1 + mat;
     for (long long q = t.tid(); q < (long long)n * k; q += t.nthreads()) Cf[q] = Cm[q] * focc[q / n];
     t.sync();
-    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.P + mat, n);
+    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.P + mat, n, GEMM_LOWER_TILES);
     t.sync();
+    team_mirror_lower(t, S.P + mat, n, 0, n);
+    t.sync();
+    TEAM_PHASE(7);
 }
 
 __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
@@ -173,7 +190,9 @@ __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPla
         Cf[q] = Cm[q] * (S.focc[ao0 + c] * S.emo[ao0 + c]);
     }
     t.sync();
-    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.W + mat, n);
+    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.W + mat, n, GEMM_LOWER_TILES);
+    t.sync();
+    team_mirror_lower(t, S.W + mat, n, 0, n);
     t.sync();
 }
 
@@ -192,7 +211,7 @@ __device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan&
     }
 }
 
-__global__ void __launch_bounds__(TEAM_THREADS) k_team(Batch B, State S, TeamPlan P, int phase) {
+__global__ void __launch_bounds__(TEAM_THREADS, 2) k_team(Batch B, State S, TeamPlan P, int phase) {
     Team g{(int)blockIdx.x, (int)gridDim.x, true};
     for (int i = 0; i < P.nbig; i++) {
         int m = P.big[i];

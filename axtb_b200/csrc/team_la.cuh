@@ -64,81 +64,125 @@ __device__ double team_sum(const Team& t, double v, double* gred) {
 
 // ---------------------------------------------------------------------------------- GEMM
 // C(MxN) = alpha op(A) op(B) + beta C; op(A) = A (M x K, lda) or A^T (A is K x M);
-// op(B) = B (K x N, ldb) or B^T (B is N x K). 64x64 tiles, k-steps of 16, 4x4 per thread.
+// op(B) = B (K x N, ldb) or B^T (B is N x K). 64x64 CTA tiles on FP64 tensor cores
+// (mma.sync m8n8k4.f64: each of the 8 warps owns a 32x16 block of 4x2 MMA tiles), k-steps of 16
+// staged through two shared-memory buffers with the next step's global loads in flight in
+// registers while the current step computes. Flags restrict the work to the non-zero part of
+// structured operands (exactly: the skipped products are zero) or of symmetric results:
+//   GEMM_A_LOWER  op(A) lower triangular: k <= row      GEMM_A_UPPER  op(A) upper: k >= row
+//   GEMM_B_UPPER  op(B) upper triangular: k <= col      GEMM_LOWER_TILES  only tiles with bi >= bj
 constexpr int GT = 64, GK = 16;
+enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8 };
+
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
 
 __device__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
-                          long long lda, const double* B, long long ldb, double beta, double* Cm, long long ldc) {
-    __shared__ double As[GK][GT + 1];
-    __shared__ double Bs[GK][GT + 1];
+                          long long lda, const double* B, long long ldb, double beta, double* Cm, long long ldc,
+                          int flags = 0) {
+    __shared__ double As[2][GK][GT + 2];
+    __shared__ double Bs[2][GK][GT + 2];
     if (M <= 0 || N <= 0) return;
     int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
-    int r = threadIdx.x & 15, c = threadIdx.x >> 4;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int wm = warp & 1, wn = warp >> 1;  // warp block: rows wm*32.., cols wn*16..
+    int lr = lane >> 2, lc = lane & 3;
+    // each thread stages 4 elements of each operand per k-step (element e = tid + 256 q, laid
+    // out along the operand's contiguous dimension)
+#define A_MM(q) (ta ? (int)(threadIdx.x + (q) * 256) / GK : (int)(threadIdx.x + (q) * 256) % GT)
+#define A_KK(q) (ta ? (int)(threadIdx.x + (q) * 256) % GK : (int)(threadIdx.x + (q) * 256) / GT)
+#define B_NN(q) (tb ? (int)(threadIdx.x + (q) * 256) % GT : (int)(threadIdx.x + (q) * 256) / GK)
+#define B_KK(q) (tb ? (int)(threadIdx.x + (q) * 256) / GT : (int)(threadIdx.x + (q) * 256) % GK)
     for (int tile = t.rank; tile < tm * tn; tile += t.size) {
         int bi = tile % tm, bj = tile / tm;
+        if ((flags & GEMM_LOWER_TILES) && bj > bi) continue;
         int row0 = bi * GT, col0 = bj * GT;
-        double acc[4][4];
+        int kb = 0, ke = K;
+        if (flags & GEMM_A_LOWER) ke = min(ke, row0 + GT);
+        if (flags & GEMM_B_UPPER) ke = min(ke, col0 + GT);
+        if (flags & GEMM_A_UPPER) kb = (row0 / GK) * GK;
+        double acc[4][2][2];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-        for (int k0 = 0; k0 < K; k0 += GK) {
-            __syncthreads();
-            for (int e = threadIdx.x; e < GT * GK; e += blockDim.x) {
-                int kk, mm;
-                if (!ta) {
-                    mm = e % GT;
-                    kk = e / GT;
-                } else {
-                    kk = e % GK;
-                    mm = e / GK;
-                }
-                int gr = row0 + mm, gk = k0 + kk;
-                double v = 0.0;
-                if (gr < M && gk < K) v = ta ? A[gk + (long long)gr * lda] : A[gr + (long long)gk * lda];
-                As[kk][mm] = v;
+            for (int j = 0; j < 2; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+        double ra[4], rb[4];
+        auto load = [&](int k0) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                int gr = row0 + A_MM(q), gk = k0 + A_KK(q);
+                ra[q] = (gr < M && gk < ke) ? (ta ? A[gk + (long long)gr * lda] : A[gr + (long long)gk * lda]) : 0.0;
+                int gc = col0 + B_NN(q), gk2 = k0 + B_KK(q);
+                rb[q] = (gc < N && gk2 < ke) ? (tb ? B[gc + (long long)gk2 * ldb] : B[gk2 + (long long)gc * ldb]) : 0.0;
             }
-            for (int e = threadIdx.x; e < GT * GK; e += blockDim.x) {
-                int kk, nn;
-                if (!tb) {
-                    kk = e % GK;
-                    nn = e / GK;
-                } else {
-                    nn = e % GT;
-                    kk = e / GT;
-                }
-                int gc = col0 + nn, gk = k0 + kk;
-                double v = 0.0;
-                if (gc < N && gk < K) v = tb ? B[gc + (long long)gk * ldb] : B[gk + (long long)gc * ldb];
-                Bs[kk][nn] = v;
+        };
+        auto store = [&](int buf) {
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                As[buf][A_KK(q)][A_MM(q)] = ra[q];
+                Bs[buf][B_KK(q)][B_NN(q)] = rb[q];
             }
-            __syncthreads();
+        };
+        __syncthreads();
+        int cur = 0;
+        if (kb < ke) {
+            load(kb);
+            store(0);
+        }
+        __syncthreads();
+        for (int k0 = kb; k0 < ke; k0 += GK) {
+            bool more = k0 + GK < ke;
+            if (more) load(k0 + GK);
 #pragma unroll
-            for (int kk = 0; kk < GK; kk++) {
-                double a[4], b[4];
+            for (int kk = 0; kk < GK; kk += 4) {
+                double af[4], bf[2];
 #pragma unroll
-                for (int i = 0; i < 4; i++) a[i] = As[kk][r + 16 * i];
+                for (int i = 0; i < 4; i++) af[i] = As[cur][kk + lc][wm * 32 + i * 8 + lr];
 #pragma unroll
-                for (int j = 0; j < 4; j++) b[j] = Bs[kk][c + 16 * j];
+                for (int j = 0; j < 2; j++) bf[j] = Bs[cur][kk + lc][wn * 16 + j * 8 + lr];
 #pragma unroll
                 for (int i = 0; i < 4; i++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                    for (int j = 0; j < 2; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+            }
+            if (more) {
+                store(cur ^ 1);
+                __syncthreads();
+                cur ^= 1;
             }
         }
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            int gc = col0 + c + 16 * j;
-            if (gc >= N) continue;
+        for (int i = 0; i < 4; i++) {
+            int gr = row0 + wm * 32 + i * 8 + lr;
+            if (gr >= M) continue;
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                int gr = row0 + r + 16 * i;
-                if (gr >= M) continue;
-                double* dst = &Cm[gr + (long long)gc * ldc];
-                double v = alpha * acc[i][j];
-                *dst = beta == 0.0 ? v : v + beta * *dst;
-            }
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    int gc = col0 + wn * 16 + j * 8 + lc * 2 + h;
+                    if (gc >= N) continue;
+                    double* dst = &Cm[gr + (long long)gc * ldc];
+                    double v = alpha * acc[i][j][h];
+                    *dst = beta == 0.0 ? v : v + beta * *dst;
+                }
         }
+    }
+}
+
+#undef A_MM
+#undef A_KK
+#undef B_NN
+#undef B_KK
+
+// A[c][i] = A[i][c] for i > c in the square block [r0, n)
+__device__ void team_mirror_lower(const Team& t, double* A, long long lda, int r0, int n) {
+    int m = n - r0;
+    for (long long q = t.tid(); q < (long long)m * m; q += t.nthreads()) {
+        int i = r0 + (int)(q % m), c = r0 + (int)(q / m);
+        if (i < c) A[i + (long long)c * lda] = A[c + (long long)i * lda];
     }
 }
 
@@ -437,9 +481,12 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
         // (4) trailing update of rows and columns q0..n-1
         int q0 = j0 + nb, mm = n - q0;
         if (mm > 0) {
-            team_gemm(t, false, true, mm, mm, nb, -1.0, V + q0, ldv, W + q0, ldv, 1.0, A + q0 + (long long)q0 * lda, lda);
+            double* Aq = A + q0 + (long long)q0 * lda;
+            team_gemm(t, false, true, mm, mm, nb, -1.0, V + q0, ldv, W + q0, ldv, 1.0, Aq, lda, GEMM_LOWER_TILES);
             t.sync();
-            team_gemm(t, false, true, mm, mm, nb, -1.0, W + q0, ldv, V + q0, ldv, 1.0, A + q0 + (long long)q0 * lda, lda);
+            team_gemm(t, false, true, mm, mm, nb, -1.0, W + q0, ldv, V + q0, ldv, 1.0, Aq, lda, GEMM_LOWER_TILES);
+            t.sync();
+            team_mirror_lower(t, A, lda, q0, n);
             t.sync();
         }
     }
