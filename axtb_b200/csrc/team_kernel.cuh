@@ -30,8 +30,7 @@ struct TeamPlan {
     int cycles;               // 1: accumulate per-phase SM cycles of mol_eigen into g_team_cycles
 };
 
-// per-phase cycle counters of the eigen phase (instrumentation, read by the profiler)
-__device__ unsigned long long g_team_cycles[16];
+// per-phase cycle counters of the eigen phase (g_team_cycles, instrumentation read by the profiler)
 #define TEAM_PHASE(k)                                                  \
     do {                                                               \
         if (P.cycles && t.tid() == 0) {                                \
@@ -116,8 +115,9 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     {
         double* Vp = wk + 2 * n + (long long)P.max_chunks * n;  // the back-transform's vb area (64 n)
         team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
-                             P.max_chunks);
+                             P.max_chunks, P.cycles != 0);
     }
+    if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..14
     TEAM_PHASE(1);
     double* emo = S.emo + ao0;
     team_bisect(t, d, e, n, emo, wk);

@@ -22,6 +22,10 @@ namespace cg = cooperative_groups;
 
 constexpr int TEAM_THREADS = 256;
 
+// SM-cycle counters of the eigen phase's parts (instrumentation, read by the profiler):
+// 0..7 the phases of the eigen step, 8..14 the parts of the tridiagonal reduction
+__device__ unsigned long long g_team_cycles[16];
+
 struct Team {
     int rank;     // CTA rank in the team
     int size;     // CTAs in the team
@@ -410,10 +414,18 @@ __device__ int team_symv_partials(const Team& t, const double* A, long long lda,
 
 __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
                                      double* V, double* W, double* vbuf, double* pbuf, double* ppart, double* gred,
-                                     int max_chunks) {
+                                     int max_chunks, bool cyc = false) {
     __shared__ double ys[64];
     const long long ldv = n;
     int nrefl = n - 2;
+    long long t0 = clock64();
+    auto tick = [&](int k) {
+        if (cyc && t.tid() == 0) {
+            long long now = clock64();
+            atomicAdd(&g_team_cycles[k], (unsigned long long)(now - t0));
+            t0 = now;
+        }
+    };
     for (int j0 = 0; j0 < nrefl; j0 += NBP) {
         int nb = min(NBP, nrefl - j0);
         for (int c = 0; c < nb; c++) {
@@ -428,6 +440,7 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
                 }
                 t.sync();
             }
+            tick(8);
             // (2) Householder vector of A[r0:n, j]
             double alpha = A[r0 + (long long)j * lda];
             double xs = 0.0;
@@ -456,11 +469,14 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
                 A[r0 + (long long)j * lda] = beta;
             }
             t.sync();
+            tick(9);
             // (3) w = tau (A v - W V^T v - V W^T v) - tau^2/2 (..) v
             if (tj != 0.0) {
                 int nch = team_symv_partials(t, A, lda, r0, n, vbuf, ppart, max_chunks);
+                tick(10);
                 team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);
                 t.sync();
+                tick(11);
                 double pv = 0.0;
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
                     double s = 0.0;
@@ -477,6 +493,7 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) W[i + c * ldv] = 0.0;
             }
             t.sync();
+            tick(12);
         }
         // (4) trailing update of rows and columns q0..n-1
         int q0 = j0 + nb, mm = n - q0;
@@ -486,8 +503,10 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
             t.sync();
             team_gemm(t, false, true, mm, mm, nb, -1.0, W + q0, ldv, V + q0, ldv, 1.0, Aq, lda, GEMM_LOWER_TILES);
             t.sync();
+            tick(13);
             team_mirror_lower(t, A, lda, q0, n);
             t.sync();
+            tick(14);
         }
     }
     if (t.tid() == 0) {
