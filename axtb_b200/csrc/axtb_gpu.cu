@@ -696,7 +696,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.pair_buf = ar.take<double>((size_t)std::max(npairT, 1LL) * 5);
     s.e_atom = ar.take<double>(natT);
     s.e_terms = ar.take<double>(natT * 5);
-    s.red = ar.take<double>((size_t)grid * 64 + 64);  // team partials: 64 per CTA
+    s.red = ar.take<double>((size_t)axg::team_red_doubles(grid));  // grid-team partials
     s.eeq_A = ar.take<double>((size_t)nsqT * 3);
     // team plan
     P.big = upI(big);

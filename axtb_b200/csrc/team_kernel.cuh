@@ -212,6 +212,8 @@ __device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan&
 }
 
 __global__ void __launch_bounds__(TEAM_THREADS, 2) k_team(Batch B, State S, TeamPlan P, int phase) {
+    if (threadIdx.x == 0) s_team_gen = 0;
+    __syncthreads();
     Team g{(int)blockIdx.x, (int)gridDim.x, true};
     for (int i = 0; i < P.nbig; i++) {
         int m = P.big[i];

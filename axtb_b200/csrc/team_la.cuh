@@ -40,11 +40,42 @@ struct Team {
     __device__ __forceinline__ int nwarps() const { return (size * blockDim.x) >> 5; }
 };
 
+// Layout of the grid team's reduction buffer `gred`: the panel dot partials (64 values x at most
+// PD_PARTS CTAs), then two alternating slots of one double per CTA for team_sum.
+constexpr int PD_PARTS = 64;
+constexpr int RED_SUM0 = 64 * PD_PARTS;
+__host__ __device__ constexpr long long team_red_doubles(int grid) { return RED_SUM0 + 2LL * grid + 64; }
+
+// Parity of the grid-team sums this CTA has made (k_team clears it at entry; every CTA makes the
+// same sequence of calls, so the parity agrees across the grid).
+__shared__ int s_team_gen;
+
+// sum of p[0..n) by one warp: lane-strided partial sums (eight loads in flight per lane), then a
+// butterfly; the order is fixed, so every lane and every CTA gets the same bits. p is read
+// through L2 (written by other CTAs before a grid barrier).
+__device__ __forceinline__ double warp_gather_sum(const double* p, int n) {
+    int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int k0 = 0; k0 < n; k0 += 256) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            int k = k0 + u * 32 + lane;
+            v[u] = k < n ? __ldcg(p + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) s += v[u];
+    }
+    return warp_sum(s);
+}
+
 // Deterministic team sum: warp sums, CTA sum in fixed warp order, then (global team) the CTA
-// partials summed in rank order by every thread. `gred` holds one double per CTA.
+// partials gathered by one warp in a fixed order. A grid team writes its partials into one of
+// two alternating slots: a CTA that runs ahead into the next sum writes the other slot while a
+// slow one still reads this one, so one grid barrier per sum suffices.
 __device__ double team_sum(const Team& t, double v, double* gred) {
     __shared__ double sred[TEAM_THREADS / 32];
-    __shared__ double sout;
+    __shared__ double sout, sall;
     v = warp_sum(v);
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     __syncthreads();
@@ -58,12 +89,18 @@ __device__ double team_sum(const Team& t, double v, double* gred) {
     __syncthreads();
     double blk = sout;
     if (!t.global) return blk;
-    if (threadIdx.x == 0) gred[t.rank] = blk;
+    double* slot = gred + RED_SUM0 + (long long)(s_team_gen & 1) * t.size;
+    if (threadIdx.x == 0) slot[t.rank] = blk;
     t.sync();
-    double s = 0.0;
-    for (int k = 0; k < t.size; k++) s += gred[k];
-    t.sync();  // gred reusable afterwards
-    return s;
+    if (threadIdx.x < 32) {
+        double s = warp_gather_sum(slot, t.size);
+        if (threadIdx.x == 0) {
+            sall = s;
+            s_team_gen++;
+        }
+    }
+    __syncthreads();
+    return sall;
 }
 
 // ---------------------------------------------------------------------------------- GEMM
@@ -250,121 +287,70 @@ __device__ void team_trinv(const Team& t, const double* L, long long ldl, double
 }
 
 // ---------------------------------------------------------------------------------- tridiagonal
-// Householder reduction of the symmetric A (full storage, n x n) to T = Q^T A Q; d, e get the
-// diagonal and subdiagonal, tau the reflector factors; reflector j (I - tau_j v v^T, v_{j+1} = 1)
-// is kept in A[j+2:n, j]. vbuf/pbuf hold n doubles; ppart holds nchunk*n partial sums.
-__device__ void team_tridiag(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
-                             double* vbuf, double* pbuf, double* ppart, double* gred, int max_chunks) {
-    for (int j = 0; j + 2 < n; j++) {
-        int r0 = j + 1, m = n - r0;  // trailing block rows/cols r0..n-1
-        double alpha = A[r0 + (long long)j * lda];
-        double xs = 0.0;
-        for (int i = r0 + 1 + t.tid(); i < n; i += t.nthreads()) xs += sq(A[i + (long long)j * lda]);
-        double xnorm2 = team_sum(t, xs, gred);
-        double beta, tj, scale;
-        if (xnorm2 == 0.0) {
-            tj = 0.0;
-            beta = alpha;
-            scale = 0.0;
-        } else {
-            beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
-            tj = (beta - alpha) / beta;
-            scale = 1.0 / (alpha - beta);
-        }
-        for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
-            double v = i == r0 ? 1.0 : A[i + (long long)j * lda] * scale;
-            vbuf[i] = v;
-            if (i > r0) A[i + (long long)j * lda] = v;
-        }
-        if (t.tid() == 0) {
-            e[j] = beta;
-            tau[j] = tj;
-            d[j] = A[j + (long long)j * lda];
-            A[r0 + (long long)j * lda] = beta;
-        }
-        t.sync();
-        if (tj != 0.0) {
-            // p = tau A v over the trailing block: warps own 32-row tiles x column chunks
-            int rt = (m + 31) / 32;
-            int nch = max(1, min(max_chunks, (t.nwarps() * 2 + rt - 1) / rt));
-            int cw = (m + nch - 1) / nch;
-            int lane = threadIdx.x & 31;
-            for (int it = t.warp(); it < rt * nch; it += t.nwarps()) {
-                int tr = it % rt, ch = it / rt;
-                int row = r0 + tr * 32 + lane;
-                int c0 = r0 + ch * cw, c1 = min(n, c0 + cw);
-                double s = 0.0;
-                if (row < n)
-                    for (int c = c0; c < c1; c++) s = fma(A[row + (long long)c * lda], vbuf[c], s);
-                if (row < n) ppart[(long long)ch * n + row] = s;
-            }
-            t.sync();
-            double pv = 0.0;
-            for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
-                double s = 0.0;
-                for (int ch = 0; ch < nch; ch++) s += ppart[(long long)ch * n + i];
-                s *= tj;
-                pbuf[i] = s;
-                pv += s * vbuf[i];
-            }
-            double dot = team_sum(t, pv, gred);
-            double K = -0.5 * tj * dot;
-            for (int i = r0 + t.tid(); i < n; i += t.nthreads()) pbuf[i] += K * vbuf[i];  // w
-            t.sync();
-            long long tot = (long long)m * m;
-            for (long long q = t.tid(); q < tot; q += t.nthreads()) {
-                int i = r0 + (int)(q % m), c = r0 + (int)(q / m);
-                A[i + (long long)c * lda] -= vbuf[i] * pbuf[c] + pbuf[i] * vbuf[c];
-            }
-            t.sync();
-        }
-    }
-    if (t.tid() == 0) {
-        if (n >= 2) {
-            d[n - 2] = A[(n - 2) + (long long)(n - 2) * lda];
-            e[n - 2] = A[(n - 1) + (long long)(n - 2) * lda];
-            tau[n - 2] = 0.0;
-        }
-        d[n - 1] = A[(n - 1) + (long long)(n - 1) * lda];
-        e[n - 1] = 0.0;
-        tau[n - 1] = 0.0;
-    }
-    t.sync();
-}
-
-// ---------------------------------------------------------------------------------- blocked
-// The same reduction in panels of NBP columns (the LAPACK dsytrd/dlatrd scheme): within a
-// panel, column j is first brought up to date with the panel's earlier reflectors, its
-// Householder vector is formed, and w = tau (A v - W (V^T v) - V (W^T v)) uses the trailing matrix
-// as it was at the start of the panel (one read-only pass, no writes); after the panel the
-// trailing matrix takes the rank-2*NBP update A -= V W^T + W V^T on GEMMs. V and W are n x NBP
-// (leading dimension n); the reflectors end up in A exactly as in team_tridiag.
+// Householder reduction of the symmetric A (n x n) to T = Q^T A Q in panels of NBP columns (the
+// LAPACK dsytrd/dlatrd scheme): d, e get the diagonal and subdiagonal, tau the reflector factors;
+// reflector j (I - tau_j v v^T, v_{j+1} = 1) is kept in A[j+2:n, j]. Within a panel, column j is
+// first brought up to date with the panel's earlier reflectors, its Householder vector is formed,
+// and w = tau (A v - W (V^T v) - V (W^T v)) uses the trailing matrix as it was at the start of the
+// panel (one read-only pass, no writes); after the panel the trailing matrix takes the rank-2*NBP
+// update A -= V W^T + W V^T on GEMMs. V and W are n x NBP (leading dimension n).
 constexpr int NBP = 32;
 
 // ys[q] = V[r0:n, q] . v (q < c) and ys[c + q] = W[r0:n, q] . v, into shared memory
 __device__ void team_panel_dots(const Team& t, const double* V, const double* W, long long ldv, const double* v, int r0,
                                 int n, int c, double* ys, double* gpart) {
+    static_assert(2 * NBP <= 64 && TEAM_THREADS == 256, "panel dots: at most 64 values, eight per warp");
     __syncthreads();
     int nq = 2 * c;
-    int m = n - r0, per = (m + t.size - 1) / t.size;
-    int rb0 = r0 + t.rank * per, rb1 = min(n, rb0 + per);
+    // a grid team splits the rows over PD_PARTS CTAs only (few partials to gather afterwards)
+    int parts = t.global ? min(t.size, PD_PARTS) : 1;
     int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int q = wid; q < nq; q += nw) {
-        const double* X = q < c ? V + (long long)q * ldv : W + (long long)(q - c) * ldv;
-        double s = 0.0;
-        for (int i = rb0 + lane; i < rb1; i += 32) s = fma(X[i], v[i], s);
-        s = warp_sum(s);
-        if (lane == 0) {
-            if (t.global) gpart[t.rank * 64 + q] = s;
-            else ys[q] = s;
+    if (t.rank < parts) {
+        int m = n - r0, per = (m + parts - 1) / parts;
+        int rb0 = r0 + t.rank * per, rb1 = min(n, rb0 + per);
+        // warp wid takes the vectors q = wid + 8u, all in one pass over its rows
+        double s[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) s[u] = 0.0;
+        for (int i = rb0 + lane; i < rb1; i += 32) {
+            double vi = v[i];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                int q = wid + u * nw;
+                if (q < nq) {
+                    const double* X = q < c ? V + (long long)q * ldv : W + (long long)(q - c) * ldv;
+                    s[u] = fma(X[i], vi, s[u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            int q = wid + u * nw;
+            double r = warp_sum(s[u]);
+            if (lane == 0 && q < nq) {
+                if (t.global) gpart[q * PD_PARTS + t.rank] = r;
+                else ys[q] = r;
+            }
         }
     }
     if (t.global) {
         t.sync();
-        if ((int)threadIdx.x < nq) {
-            double s = 0.0;
-            for (int r = 0; r < t.size; r++) s += gpart[r * 64 + threadIdx.x];
-            ys[threadIdx.x] = s;
+        // warp wid gathers q = wid + 8u: lane holds parts lane and lane + 32; the butterfly gives
+        // every CTA the same sum
+        double g[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            int q = wid + u * nw;
+            const double* gp = gpart + q * PD_PARTS;
+            double a0 = (q < nq && lane < parts) ? __ldcg(gp + lane) : 0.0;
+            double a1 = (q < nq && lane + 32 < parts) ? __ldcg(gp + lane + 32) : 0.0;
+            g[u] = a0 + a1;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            int q = wid + u * nw;
+            double r = warp_sum(g[u]);
+            if (lane == 0 && q < nq) ys[q] = r;
         }
     }
     __syncthreads();
@@ -430,22 +416,24 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
         int nb = min(NBP, nrefl - j0);
         for (int c = 0; c < nb; c++) {
             int j = j0 + c, r0 = j + 1;
-            // (1) column j brought up to date with the panel's earlier reflectors
-            if (c > 0) {
-                for (int i = j + t.tid(); i < n; i += t.nthreads()) {
+            // (1) column j brought up to date with the panel's earlier reflectors, in the same pass
+            // as the squared norm of A[r0+1:n, j] for (2) its Householder vector; the team sum's
+            // barrier publishes the updated column
+            double xs = 0.0;
+            for (int i = j + t.tid(); i < n; i += t.nthreads()) {
+                double a = A[i + (long long)j * lda];
+                if (c > 0) {
                     double s = 0.0;
                     for (int q = 0; q < c; q++)
                         s += V[i + q * ldv] * W[j + q * ldv] + W[i + q * ldv] * V[j + q * ldv];
-                    A[i + (long long)j * lda] -= s;
+                    a -= s;
+                    A[i + (long long)j * lda] = a;
                 }
-                t.sync();
+                if (i > r0) xs += sq(a);
             }
             tick(8);
-            // (2) Householder vector of A[r0:n, j]
-            double alpha = A[r0 + (long long)j * lda];
-            double xs = 0.0;
-            for (int i = r0 + 1 + t.tid(); i < n; i += t.nthreads()) xs += sq(A[i + (long long)j * lda]);
             double xnorm2 = team_sum(t, xs, gred);
+            double alpha = A[r0 + (long long)j * lda];
             double beta, tj, scale;
             if (xnorm2 == 0.0) {
                 tj = 0.0;
@@ -474,8 +462,7 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
             if (tj != 0.0) {
                 int nch = team_symv_partials(t, A, lda, r0, n, vbuf, ppart, max_chunks);
                 tick(10);
-                team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);
-                t.sync();
+                team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);  // its barrier also publishes ppart
                 tick(11);
                 double pv = 0.0;
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {

@@ -67,6 +67,27 @@ def test_batch_equals_single_and_oracle(engine):
         assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
 
 
+def test_grid_team_path_matches_oracle(engine, golden, monkeypatch):
+    """Molecules from AXTB_TEAM_BIG_NAO AOs on run their dense algebra on the whole cooperative
+    grid (grid-wide barriers and cross-CTA reductions) instead of one CTA; lowering the threshold
+    sends small molecules down that path, in the same launch as one-CTA molecules."""
+    from axtb_b200 import structures as S
+
+    monkeypatch.setenv("AXTB_TEAM_BIG_NAO", "100")
+    z0, x0, q0, u0 = _mol(golden, "struct-taxol")
+    mols = [(z0, x0, q0, u0), S.water_cluster(20, 3, dims=(5, 2, 2)) + (0.0, None),
+            S.alkane(8, seed=2) + (0.0, None)]
+    b = engine.Batch(mols, accuracy=1e-6)
+    res = b.run(gradient=True)
+    again = b.run(gradient=True)  # the cross-CTA reductions have a fixed order: same bits
+    for (z, x, q, u), r, r2 in zip(mols, res, again):
+        assert r.energy == r2.energy and np.array_equal(r.gradient, r2.gradient)
+        ref = O.singlepoint(z, x, q, u, accuracy=1e-6)
+        assert r.status == 0
+        assert abs(r.energy - ref["energy"]) < E_TOL, (r.energy, ref["energy"])
+        assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
+
+
 def test_golden_energies(engine, golden):
     ids = [c for c in golden if c.startswith("el-")][:40] + ["struct-anthracene2", "struct-tyr-xab",
                                                              "struct-s229-cl", "struct-beni-acetone"]
