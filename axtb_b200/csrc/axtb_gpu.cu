@@ -241,6 +241,7 @@ struct AxtbBatch {
     };
     bool profiling = false;
     double team_cycles[16] = {0};
+    std::vector<double> eigen_ms;  // each eigen launch of the last profiled run (ms)
     vector<Rec> recs;
     std::map<std::string, Acc> prof;
     int* h_act = nullptr;          // pinned copy of the active flags
@@ -286,7 +287,6 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     m_pair0.resize(nmol);
     m_vec0.resize(nmol);
     hist_cap = std::min(o.max_iter, nmol > 16 ? 64 : 128);
-    const int MAXCH = 16;
     natT = nshT = naoT = 0;
     nnT = npairT = npdT = nvecT = nsqT = ntiles = nwk = nhist = 0;
     for (int m = 0; m < nmol; m++) {
@@ -322,7 +322,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         long long nt = (n + 31) / 32;
         ntiles += nt * nt;
         long long nw = std::max(n, 64LL);
-        nwk += (2 + MAXCH) * nw + 64LL * nw + 2 * 64 * 64 + 2 * 64LL * nw + 64LL * nw + 64;
+        nwk += (2LL + axg::symv_slots((int)n)) * nw + 64LL * nw + 2 * 64 * 64 + 2 * 64LL * nw + 64LL * nw + 64;
     }
     // atoms / shells / AOs
     vector<int> a_Z(natT), a_mol(natT), a_sh0(natT), a_nsh(natT), a_ao0(natT), a_sp(natT);
@@ -709,7 +709,6 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     P.eeq_rhs = ar.take<double>(natT);
     P.eeq_q = ar.take<double>(natT);
     P.eeq_plane = nsqT;
-    P.max_chunks = MAXCH;
     d_wt = ar.take<double>(std::max(nsqT, 1LL));
     d_tt = ar.take<double>(std::max(nsqT, 1LL));
     d_eatm = ar.take<double>(nmol);
@@ -834,9 +833,11 @@ void AxtbBatch::resolve_profile() {
     unsigned long long cyc[16];
     CK(cudaMemcpyFromSymbol(cyc, axg::g_team_cycles, sizeof cyc));
     for (int k = 0; k < 16; k++) team_cycles[k] += (double)cyc[k];
+    eigen_ms.clear();
     for (auto& r : recs) {
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+        if (std::strcmp(r.name, "team_eigen") == 0) eigen_ms.push_back(ms);
         auto& a = prof[r.name];
         a.launches += 1;
         a.ms += ms;
@@ -1085,7 +1086,6 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.P = d_density;
     B.nmol = 1;
     B.kt = kt;
-    P.max_chunks = 16;
     axg::k_density_static<<<1, axg::TEAM_THREADS, 0, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta, d_status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

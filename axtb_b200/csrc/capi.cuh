@@ -325,12 +325,11 @@ int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
     // SM-cycle shares of the eigen phase's parts (one-CTA teams)
     static const char* PH[8] = {"transform", "tridiagonal", "bisection", "fermi", "inverse_iteration",
                                 "back_transform", "c_matrix", "density"};
-    // slots 8..14: parts of the tridiagonal reduction (counted instead of slot 1)
-    static const char* TP[7] = {"column_update", "householder", "symv", "panel_dots", "combine", "trailing_gemm",
-                                "mirror"};
+    // slots 8..13: parts of the tridiagonal reduction (counted instead of slot 1)
+    static const char* TP[6] = {"column_update", "householder", "symv", "panel_dots", "combine", "trailing_gemm"};
     double ph[8], tc = 0.0, tt = 0.0;
     for (int k = 0; k < 8; k++) ph[k] = b->team_cycles[k];
-    for (int k = 8; k < 15; k++) tt += b->team_cycles[k];
+    for (int k = 8; k < 14; k++) tt += b->team_cycles[k];
     ph[1] += tt;
     for (int k = 0; k < 8; k++) tc += ph[k];
     s += "}, \"team_eigen_phases\": {";
@@ -340,14 +339,20 @@ int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
         s += tmp;
     }
     s += "}, \"tridiagonal_parts\": {";
-    for (int k = 0; k < 7; k++) {
+    for (int k = 0; k < 6; k++) {
         char tmp[96];
         std::snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", k ? ", " : "", TP[k],
                       tt > 0 ? b->team_cycles[8 + k] / tt : 0.0);
         s += tmp;
     }
+    s += "}, \"eigen_launch_ms\": [";
+    for (size_t k = 0; k < b->eigen_ms.size(); k++) {
+        char tmp[32];
+        std::snprintf(tmp, sizeof tmp, "%s%.3f", k ? ", " : "", b->eigen_ms[k]);
+        s += tmp;
+    }
     char tail[160];
-    std::snprintf(tail, sizeof tail, "}, \"h2d_bytes\": %lld, \"d2h_bytes\": %lld, \"grid\": %d}", b->h2d_bytes,
+    std::snprintf(tail, sizeof tail, "], \"h2d_bytes\": %lld, \"d2h_bytes\": %lld, \"grid\": %d}", b->h2d_bytes,
                   b->d2h_bytes, b->grid);
     s += tail;
     if (buf && len > 0) {

@@ -26,7 +26,6 @@ struct TeamPlan {
     double* eeq_rhs;          // natT
     double* eeq_q;            // natT: EEQ charges
     long long eeq_plane;      // size of one EEQ plane (sum nat^2)
-    int max_chunks;
     int cycles;               // 1: accumulate per-phase SM cycles of mol_eigen into g_team_cycles
 };
 
@@ -97,13 +96,11 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* X = S.scr1 + mat;
     double* Fp = S.Fp + mat;
     long long t0__ = clock64();
-    // F' = L^-1 F L^-T, symmetrised
-    // (L^-1 is lower triangular; F' is symmetric: its lower tiles are computed and mirrored)
+    // F' = L^-1 F L^-T (L^-1 is lower triangular; F' is symmetric and only its lower triangle is
+    // used: the tiles on and below the diagonal are computed)
     team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n, GEMM_A_LOWER);
     t.sync();
     team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n, GEMM_B_UPPER | GEMM_LOWER_TILES);
-    t.sync();
-    team_mirror_lower(t, Fp, n, 0, n);
     t.sync();
     TEAM_PHASE(0);
     double* d = S.dtri + ao0;
@@ -112,12 +109,13 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* vbuf = wk;
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
+    const int nsl = symv_slots(n);
     {
-        double* Vp = wk + 2 * n + (long long)P.max_chunks * n;  // the back-transform's vb area (64 n)
+        double* Vp = wk + 2 * n + (long long)nsl * n;  // the back-transform's vb area (64 n)
         team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
-                             P.max_chunks, P.cycles != 0);
+                             P.cycles != 0);
     }
-    if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..14
+    if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     TEAM_PHASE(1);
     double* emo = S.emo + ao0;
     team_bisect(t, d, e, n, emo, wk);
@@ -158,7 +156,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     team_invit(t, d, e, emo, n, k, Zm, n, S.scr1 + mat, S.scr2 + mat, S.scr3 + mat, S.piv + mat, S.P + mat, &S.status[m]);
     TEAM_PHASE(4);
     // back-transform: vb (n x 64), tb, gm (64 x 64), y, y2 (64 x k)
-    double* vb = wk + 2 * n + (long long)P.max_chunks * n;
+    double* vb = wk + 2 * n + (long long)nsl * n;
     double* tb = vb + 64LL * n;
     double* gm = tb + 64 * 64;
     double* y = gm + 64 * 64;

@@ -23,7 +23,7 @@ namespace cg = cooperative_groups;
 constexpr int TEAM_THREADS = 256;
 
 // SM-cycle counters of the eigen phase's parts (instrumentation, read by the profiler):
-// 0..7 the phases of the eigen step, 8..14 the parts of the tridiagonal reduction
+// 0..7 the phases of the eigen step, 8..13 the parts of the tridiagonal reduction
 __device__ unsigned long long g_team_cycles[16];
 
 struct Team {
@@ -356,51 +356,105 @@ __device__ void team_panel_dots(const Team& t, const double* V, const double* W,
     __syncthreads();
 }
 
-// partial sums of A[r0:n, r0:n] v over column chunks: warps own 64-row tiles (two rows per lane)
-// x column chunks, four columns per step with independent accumulators; ppart[ch * n + row]
-__device__ int team_symv_partials(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
-                                  double* ppart, int max_chunks) {
+// Column-chunk slots of the symv partial sums for an n x n matrix (tiles of 64 plus one).
+__host__ __device__ constexpr int symv_slots(int n) { return (n + 63) / 64 + 1; }
+
+// y = A[r0:n, r0:n] v from the lower triangle only (A symmetric; the strict upper triangle is
+// never read and may hold stale values). The trailing matrix is cut into 64 x 64 tiles (blocks
+// counted from r0, bi >= bj); a warp takes a tile, each lane two of its rows (lane, lane + 32),
+// and reads 16 columns per round (32 loads in flight per lane). A tile adds A_ic v_c to the rows
+// of block bi (slot bj) and, strictly below the diagonal, A_ic v_i to the rows of block bj
+// (slot bi, or the extra slot rt for a diagonal tile): every (slot, row) is written exactly once,
+// so summing the rt + 1 slots of a row has a fixed order. ppart[slot * n + row]; returns rt + 1.
+__device__ int team_symv_lower(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
+                               double* ppart) {
     int m = n - r0;
     int rt = (m + 63) / 64;
-    int nch = max(1, min(max_chunks, (t.nwarps() * 2 + rt - 1) / rt));
-    int cw = (m + nch - 1) / nch;
+    int ntile = rt * (rt + 1) / 2;
     int lane = threadIdx.x & 31;
-    for (int it = t.warp(); it < rt * nch; it += t.nwarps()) {
-        int tr = it % rt, ch = it / rt;
-        int ra = r0 + tr * 64 + lane, rb = ra + 32;
-        bool oka = ra < n, okb = rb < n;
-        int la = oka ? ra : n - 1, lb = okb ? rb : n - 1;
-        int c0 = r0 + ch * cw, c1 = min(n, c0 + cw);
-        double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-        int c = c0;
-        for (; c + 3 < c1; c += 4) {
-            const double* p0 = A + (long long)c * lda;
-            double x0 = p0[la], x1 = p0[lda + la], x2 = p0[2 * lda + la], x3 = p0[3 * lda + la];
-            double y0 = p0[lb], y1 = p0[lda + lb], y2 = p0[2 * lda + lb], y3 = p0[3 * lda + lb];
-            double v0 = v[c], v1 = v[c + 1], v2 = v[c + 2], v3 = v[c + 3];
-            a0 = fma(x0, v0, a0);
-            a1 = fma(x1, v1, a1);
-            a0 = fma(x2, v2, a0);
-            a1 = fma(x3, v3, a1);
-            b0 = fma(y0, v0, b0);
-            b1 = fma(y1, v1, b1);
-            b0 = fma(y2, v2, b0);
-            b1 = fma(y3, v3, b1);
+    for (int it = t.warp(); it < ntile; it += t.nwarps()) {
+        // it = bi (bi + 1) / 2 + bj
+        int bi = (int)((sqrt(8.0 * it + 1.0) - 1.0) * 0.5);
+        while ((bi + 1) * (bi + 2) / 2 <= it) bi++;
+        while (bi * (bi + 1) / 2 > it) bi--;
+        int bj = it - bi * (bi + 1) / 2;
+        bool diag = bi == bj;
+        int i0 = r0 + bi * 64, c0 = r0 + bj * 64, c1 = min(n, c0 + 64);
+        int ia = i0 + lane, ib = ia + 32;
+        bool oka = ia < n, okb = ib < n;
+        int la = oka ? ia : n - 1, lb = okb ? ib : n - 1;
+        double va = oka ? v[ia] : 0.0, vb = okb ? v[ib] : 0.0;
+        double ra = 0.0, rb = 0.0;
+        int tslot = diag ? rt : bi;
+        for (int cb = c0; cb < c1; cb += 16) {
+            double xa[16], xb[16];
+#pragma unroll
+            for (int u = 0; u < 16; u++) {
+                const double* col = A + (long long)min(cb + u, n - 1) * lda;
+                xa[u] = col[la];
+                xb[u] = col[lb];
+            }
+            double p[16];
+#pragma unroll
+            for (int u = 0; u < 16; u++) {
+                int c = cb + u;
+                bool okc = c < c1;
+                double vc = okc ? v[c] : 0.0;
+                // lower triangle of the tile, rows and columns inside the matrix
+                double a = (oka && okc && (!diag || ia >= c)) ? xa[u] : 0.0;
+                double b = (okb && okc && (!diag || ib >= c)) ? xb[u] : 0.0;
+                ra = fma(a, vc, ra);
+                rb = fma(b, vc, rb);
+                double ta = (diag && ia == c) ? 0.0 : a;  // transposed part: strictly below
+                double tb = (diag && ib == c) ? 0.0 : b;
+                p[u] = fma(tb, vb, ta * va);
+            }
+            // reduce-scatter of the 16 column partials over the warp: after the four halving
+            // steps lane holds column u = 8 b4 + 4 b3 + 2 b2 + b1 (b_k = bit k of the lane)
+            double q8[8], q4[4], q2[2];
+            {
+                bool h = (lane >> 4) & 1;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    double r = __shfl_xor_sync(0xffffffffu, h ? p[k] : p[8 + k], 16);
+                    q8[k] = (h ? p[8 + k] : p[k]) + r;
+                }
+            }
+            {
+                bool h = (lane >> 3) & 1;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    double r = __shfl_xor_sync(0xffffffffu, h ? q8[k] : q8[4 + k], 8);
+                    q4[k] = (h ? q8[4 + k] : q8[k]) + r;
+                }
+            }
+            {
+                bool h = (lane >> 2) & 1;
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    double r = __shfl_xor_sync(0xffffffffu, h ? q4[k] : q4[2 + k], 4);
+                    q2[k] = (h ? q4[2 + k] : q4[k]) + r;
+                }
+            }
+            double cs;
+            {
+                bool h = (lane >> 1) & 1;
+                double r = __shfl_xor_sync(0xffffffffu, h ? q2[0] : q2[1], 2);
+                cs = (h ? q2[1] : q2[0]) + r;
+            }
+            cs += __shfl_xor_sync(0xffffffffu, cs, 1);
+            int cu = cb + ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+            if ((lane & 1) == 0 && cu < c1) ppart[(long long)tslot * n + cu] = cs;
         }
-        for (; c < c1; c++) {
-            double vc = v[c];
-            a0 = fma(A[la + (long long)c * lda], vc, a0);
-            b0 = fma(A[lb + (long long)c * lda], vc, b0);
-        }
-        if (oka) ppart[(long long)ch * n + ra] = a0 + a1;
-        if (okb) ppart[(long long)ch * n + rb] = b0 + b1;
+        if (oka) ppart[(long long)bj * n + ia] = ra;
+        if (okb) ppart[(long long)bj * n + ib] = rb;
     }
-    return nch;
+    return rt + 1;
 }
 
 __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
                                      double* V, double* W, double* vbuf, double* pbuf, double* ppart, double* gred,
-                                     int max_chunks, bool cyc = false) {
+                                     bool cyc = false) {
     __shared__ double ys[64];
     const long long ldv = n;
     int nrefl = n - 2;
@@ -460,7 +514,7 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
             tick(9);
             // (3) w = tau (A v - W V^T v - V W^T v) - tau^2/2 (..) v
             if (tj != 0.0) {
-                int nch = team_symv_partials(t, A, lda, r0, n, vbuf, ppart, max_chunks);
+                int nch = team_symv_lower(t, A, lda, r0, n, vbuf, ppart);
                 tick(10);
                 team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);  // its barrier also publishes ppart
                 tick(11);
@@ -491,9 +545,6 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
             team_gemm(t, false, true, mm, mm, nb, -1.0, W + q0, ldv, V + q0, ldv, 1.0, Aq, lda, GEMM_LOWER_TILES);
             t.sync();
             tick(13);
-            team_mirror_lower(t, A, lda, q0, n);
-            t.sync();
-            tick(14);
         }
     }
     if (t.tid() == 0) {
