@@ -20,7 +20,7 @@ AXTB_ERR_NUMERICAL = 4
 AXTB_ERR_DEVICE = 5
 
 DBG = {"cn": 0, "overlap": 1, "h0": 2, "dipole": 3, "quadrupole": 4, "density": 5, "fock": 6, "emo": 7,
-       "focc": 8, "wdensity": 9, "eeq": 10, "linv": 11}
+       "focc": 8, "wdensity": 9, "eeq": 10, "linv": 11, "eigen_cycles": 12}
 
 
 class AxtbOptions(C.Structure):

@@ -208,7 +208,7 @@ class Batch:
         z, _ = self.mols[mol]
         nat = len(z)
         nsh, nao = basis_size(z)
-        size = {"cn": nat, "eeq": nat, "emo": nao, "focc": nao, "dipole": 3 * nao * nao,
+        size = {"cn": nat, "eeq": nat, "emo": nao, "focc": nao, "eigen_cycles": 1, "dipole": 3 * nao * nao,
                 "quadrupole": 6 * nao * nao}.get(what, nao * nao)
         out = np.zeros(size)
         rc = _lib.load().axtb_gpu_batch_debug(self._b, mol, _lib.DBG[what], _ptr(out))

@@ -515,6 +515,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addD((size_t)naoT * 11);
     addD((size_t)nvecT * 4 + (size_t)nhist * 2 + (size_t)nmol * hist_cap * hist_cap * 2 + (size_t)nmol * hist_cap);
     addD((size_t)nmol * 14);
+    addD((size_t)nmol);  // per-molecule eigen cycles
     addD((size_t)natT * 5 + (size_t)std::max(npairT, 1LL) * 5 + natT + natT * 5);
     addD((size_t)grid * 64 + 64);
     addD((size_t)nsqT * 3 + natT * 2);
@@ -696,6 +697,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.pair_buf = ar.take<double>((size_t)std::max(npairT, 1LL) * 5);
     s.e_atom = ar.take<double>(natT);
     s.e_terms = ar.take<double>(natT * 5);
+    s.mol_cyc = ar.take<double>(nmol);
     s.red = ar.take<double>((size_t)axg::team_red_doubles(grid));  // grid-team partials
     s.eeq_A = ar.take<double>((size_t)nsqT * 3);
     // team plan

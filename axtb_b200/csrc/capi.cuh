@@ -391,6 +391,7 @@ int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out) {
             case AXTB_DBG_WDENSITY: cp(b->S.W + mat, n2); break;
             case AXTB_DBG_EEQ: cp(b->P.eeq_q + a0, nat); break;
             case AXTB_DBG_LINV: cp(b->S.Linv + mat, n2); break;
+            case AXTB_DBG_EIGEN_CYCLES: cp(b->S.mol_cyc + mol, 1); break;
             default: throw Fail(AXTB_ERR_INPUT, "unknown debug quantity");
         }
         CK(cudaStreamSynchronize(b->st));

@@ -100,6 +100,7 @@ struct State {
     double *grad, *dedcn, *dedcn_d4;  // natT*3, natT, natT
     double* pair_buf;  // npairT*8: per atom-pair gradient partials
     double* e_atom;    // natT
+    double* mol_cyc;   // nmol: SM cycles of each molecule's last eigen phase (profiling runs)
     double* e_terms;   // natT*5: ES2, ES3, AES, D4 two-body, band per atom
     // cooperative scratch
     double* red;       // reduction partials (grid-size * 8)

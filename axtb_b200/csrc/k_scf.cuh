@@ -360,8 +360,11 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
     }
     __syncthreads();
     if (s_done) return;
-    // ---- Broyden step
-    int iter = ++S.iter[m];
+    // ---- Broyden step (one thread advances the step counter; every thread reads it back)
+    __shared__ int s_iter;
+    if (tid == 0) s_iter = ++S.iter[m];
+    __syncthreads();
+    int iter = s_iter;
     double alpha = B.damping;
     if (iter == 1) {
         for (int i = tid; i < dim; i += nthr) {

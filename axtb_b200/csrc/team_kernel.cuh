@@ -45,9 +45,9 @@ __device__ void mol_overlap(const Team& t, const Batch& B, State& S, const TeamP
     double* L = S.scr1 + mat;
     for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) L[e] = S.S[mat + e];
     t.sync();
-    bool ok = team_cholesky(t, L, n, n);
-    if (!ok && t.tid() == 0) atomicOr(&S.status[m], ST_NOT_PD);
     double* tmp = P.wk + P.m_wk0[m];
+    bool ok = team_cholesky(t, L, n, n, tmp);
+    if (!ok && t.tid() == 0) atomicOr(&S.status[m], ST_NOT_PD);
     team_trinv(t, L, n, S.Linv + mat, n, n, tmp);
 }
 
@@ -57,8 +57,8 @@ __device__ void mol_eeq(const Team& t, const Batch& B, State& S, const TeamPlan&
     double* A = S.eeq_A + o;
     double* Li = S.eeq_A + P.eeq_plane + o;
     double* Ji = S.eeq_A + 2 * P.eeq_plane + o;
-    bool ok = team_cholesky(t, A, n, n);
     double* tmp = P.wk + P.m_wk0[m];
+    bool ok = team_cholesky(t, A, n, n, tmp);
     team_trinv(t, A, n, Li, n, n, tmp);
     // J^-1 = L^-T L^-1
     team_gemm(t, true, false, n, n, n, 1.0, Li, n, Li, n, 0.0, Ji, n);
@@ -95,7 +95,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* Linv = S.Linv + mat;
     double* X = S.scr1 + mat;
     double* Fp = S.Fp + mat;
-    long long t0__ = clock64();
+    long long t0__ = clock64(), tstart = t0__;
     // F' = L^-1 F L^-T (L^-1 is lower triangular; F' is symmetric and only its lower triangle is
     // used: the tiles on and below the diagonal are computed)
     team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n, GEMM_A_LOWER);
@@ -176,6 +176,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     team_mirror_lower(t, S.P + mat, n, 0, n);
     t.sync();
     TEAM_PHASE(7);
+    if (P.cycles && t.tid() == 0) S.mol_cyc[m] = (double)(clock64() - tstart);
 }
 
 __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {

@@ -7,7 +7,7 @@
 // quantities of the reference's dense algebra (crates/base/src/linalg/eigen.rs: Cholesky of S,
 // the reduced matrix L^-1 F L^-T, its eigenvalues and occupied eigenvectors, C = L^-T U; and
 // crates/base/src/linalg/density.rs: P = C diag(f) C^T) with B200-friendly algorithms:
-// right-looking Cholesky, a row-block triangular inverse on GEMMs, Householder
+// blocked right-looking Cholesky, a row-block triangular inverse on GEMMs, Householder
 // tridiagonalisation with 2-D split symmetric matrix-vector products, Sturm-count bisection for
 // all eigenvalues (one thread per eigenvalue), inverse iteration for the occupied vectors (one
 // thread per vector, re-orthogonalised within clusters of close eigenvalues) and the blocked
@@ -111,9 +111,17 @@ __device__ double team_sum(const Team& t, double v, double* gred) {
 // registers while the current step computes. Flags restrict the work to the non-zero part of
 // structured operands (exactly: the skipped products are zero) or of symmetric results:
 //   GEMM_A_LOWER  op(A) lower triangular: k <= row      GEMM_A_UPPER  op(A) upper: k >= row
-//   GEMM_B_UPPER  op(B) upper triangular: k <= col      GEMM_LOWER_TILES  only tiles with bi >= bj
+//   GEMM_B_UPPER  op(B) upper triangular: k <= col      GEMM_B_LOWER  op(B) lower: k >= col
+//   GEMM_LOWER_TILES  only tiles with bi >= bj
 constexpr int GT = 64, GK = 16;
-enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8 };
+enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8, GEMM_B_LOWER = 16 };
+
+// One shared-memory work area per CTA, used in turn (never at the same time, each user starting
+// and ending at a CTA barrier) by the GEMM's staging buffers and the Cholesky's diagonal block.
+constexpr int CB = 64;
+constexpr int SMEM_WORK = 2 * 2 * GK * (GT + 2);
+static_assert(CB * (CB + 1) <= SMEM_WORK, "diagonal block fits the GEMM staging area");
+__shared__ __align__(16) double s_work[SMEM_WORK];
 
 __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -121,11 +129,11 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__device__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
+__device__ __noinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
                           long long lda, const double* B, long long ldb, double beta, double* Cm, long long ldc,
                           int flags = 0) {
-    __shared__ double As[2][GK][GT + 2];
-    __shared__ double Bs[2][GK][GT + 2];
+    auto& As = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work);
+    auto& Bs = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work + 2 * GK * (GT + 2));
     if (M <= 0 || N <= 0) return;
     int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -144,7 +152,8 @@ __device__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, 
         int kb = 0, ke = K;
         if (flags & GEMM_A_LOWER) ke = min(ke, row0 + GT);
         if (flags & GEMM_B_UPPER) ke = min(ke, col0 + GT);
-        if (flags & GEMM_A_UPPER) kb = (row0 / GK) * GK;
+        if (flags & GEMM_A_UPPER) kb = max(kb, (row0 / GK) * GK);
+        if (flags & GEMM_B_LOWER) kb = max(kb, (col0 / GK) * GK);
         double acc[4][2][2];
 #pragma unroll
         for (int i = 0; i < 4; i++)
@@ -228,59 +237,126 @@ __device__ void team_mirror_lower(const Team& t, double* A, long long lda, int r
 }
 
 // ---------------------------------------------------------------------------------- Cholesky
-// In-place lower Cholesky of the n x n SPD matrix A (the strict upper triangle is zeroed).
-// Returns false (on every thread) when a pivot is not positive.
-__device__ bool team_cholesky(const Team& t, double* A, int n, long long lda) {
+// Blocked right-looking Cholesky and triangular inverse in panels of CB columns. The CB x CB
+// diagonal block is factored (and inverted) in shared memory by the team's first CTA; the panel
+// and the trailing matrix are DMMA GEMMs: a team barrier every few GEMMs instead of two per column.
+#define s_tri (*reinterpret_cast<double(*)[CB][CB + 1]>(s_work))
+
+// the lower triangle of the nb x nb block at Bp (leading dimension ld) into s_tri (rest zero)
+__device__ void cta_load_lower(const double* Bp, long long ld, int nb) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < CB * CB; e += blockDim.x) {
+        int r = e % CB, c = e / CB;
+        s_tri[r][c] = (r < nb && c < nb && r >= c) ? Bp[r + (long long)c * ld] : 0.0;
+    }
+    __syncthreads();
+}
+
+// in-place lower Cholesky of the block in s_tri (unblocked, right-looking); false (on every
+// thread) when a pivot is not positive
+__device__ bool cta_potrf(int nb) {
     bool ok = true;
-    for (int j = 0; j < n; j++) {
-        double ajj = A[j + (long long)j * lda];
-        if (!(ajj > 0.0)) {
+    for (int j = 0; j < nb; j++) {
+        double p = s_tri[j][j];
+        if (!(p > 0.0)) {
             ok = false;
-            ajj = 1.0;
+            p = 1.0;
         }
-        double ljj = sqrt(ajj);
-        double inv = 1.0 / ljj;
-        for (int i = j + 1 + t.tid(); i < n; i += t.nthreads()) A[i + (long long)j * lda] *= inv;
-        t.sync();
-        if (t.tid() == 0) A[j + (long long)j * lda] = ljj;
-        int m = n - j - 1;
-        long long tot = (long long)m * m;
-        for (long long e = t.tid(); e < tot; e += t.nthreads()) {
-            int i = j + 1 + (int)(e % m), c = j + 1 + (int)(e / m);
-            if (i < c) continue;
-            A[i + (long long)c * lda] -= A[i + (long long)j * lda] * A[c + (long long)j * lda];
+        double ljj = sqrt(p), inv = 1.0 / ljj;
+        __syncthreads();  // the pivot has been read
+        for (int r = j + 1 + threadIdx.x; r < nb; r += blockDim.x) s_tri[r][j] *= inv;
+        if (threadIdx.x == 0) s_tri[j][j] = ljj;
+        __syncthreads();
+        int m = nb - j - 1;
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
+            int r = j + 1 + e % m, c = j + 1 + e / m;
+            if (r >= c) s_tri[r][c] -= s_tri[r][j] * s_tri[c][j];
+        }
+        __syncthreads();
+    }
+    return ok;
+}
+
+// in-place inverse of the lower triangular block in s_tri (LAPACK dtrti2 order: columns from the
+// last, x <- -T x / l_jj with T the already inverted trailing block)
+__device__ void cta_trtri(int nb) {
+    for (int j = nb - 1; j >= 0; j--) {
+        double d = 1.0 / s_tri[j][j];
+        int r = j + 1 + threadIdx.x;
+        double y = 0.0;
+        if (r < nb)
+            for (int q = j + 1; q <= r; q++) y += s_tri[r][q] * s_tri[q][j];
+        __syncthreads();
+        if (r < nb) s_tri[r][j] = -d * y;
+        if (threadIdx.x == 0) s_tri[j][j] = d;
+        __syncthreads();
+    }
+}
+
+// In-place lower Cholesky of the n x n SPD matrix A (the strict upper triangle is zeroed).
+// Returns false (on every thread) when a pivot is not positive. scr holds CB x CB + 1 doubles.
+__device__ __noinline__ bool team_cholesky(const Team& t, double* A, int n, long long lda, double* scr) {
+    bool ok = true;  // kept by the first CTA, published in scr[CB * CB] at the end
+    for (int k0 = 0; k0 < n; k0 += CB) {
+        int nb = min(CB, n - k0), m2 = n - k0 - nb;
+        double* A11 = A + k0 + (long long)k0 * lda;
+        if (t.rank == 0) {
+            cta_load_lower(A11, lda, nb);
+            ok = cta_potrf(nb) && ok;
+            for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+                int r = e % nb, c = e / nb;
+                if (r >= c) A11[r + (long long)c * lda] = s_tri[r][c];
+            }
+            if (m2 > 0) {
+                cta_trtri(nb);
+                for (int e = threadIdx.x; e < CB * CB; e += blockDim.x) {
+                    int r = e % CB, c = e / CB;
+                    scr[e] = (r >= c) ? s_tri[r][c] : 0.0;
+                }
+            }
         }
         t.sync();
+        if (m2 > 0) {
+            double* A21 = A11 + nb;
+            double* A22 = A21 + (long long)nb * lda;
+            // L21 = A21 L11^-T, in place: an output tile (64 rows x nb <= 64 columns) reads only
+            // its own rows of A21, all of them before its first store
+            team_gemm(t, false, true, m2, nb, nb, 1.0, A21, lda, scr, CB, 0.0, A21, lda, GEMM_B_UPPER);
+            t.sync();
+            team_gemm(t, false, true, m2, m2, nb, -1.0, A21, lda, A21, lda, 1.0, A22, lda, GEMM_LOWER_TILES);
+            t.sync();
+        }
     }
     for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) {
         int i = (int)(e % n), c = (int)(e / n);
         if (i < c) A[i + (long long)c * lda] = 0.0;
     }
+    if (t.tid() == 0) scr[CB * CB] = ok ? 1.0 : 0.0;
     t.sync();
-    return ok;
+    return scr[CB * CB] != 0.0;
 }
 
-// Linv = L^-1 for lower triangular L (n x n), row blocks of 64: Linv[I, :] = L_II^-1 (E_I -
-// L[I, 0:i0] Linv[0:i0, :]); `tmp` holds 64 x n.
-__device__ void team_trinv(const Team& t, const double* L, long long ldl, double* Linv, long long ldi, int n, double* tmp) {
+// Linv = L^-1 for lower triangular L (n x n), row blocks of CB: the diagonal block is inverted in
+// shared memory, then Linv[I, 0:i0] = L_II^-1 (-L[I, 0:i0] Linv[0:i0, 0:i0]) on two GEMMs;
+// `tmp` holds CB x n.
+__device__ __noinline__ void team_trinv(const Team& t, const double* L, long long ldl, double* Linv, long long ldi, int n, double* tmp) {
     for (long long e = t.tid(); e < (long long)n * n; e += t.nthreads()) Linv[(e % n) + (e / n) * ldi] = 0.0;
     t.sync();
-    for (int i0 = 0; i0 < n; i0 += GT) {
-        int nb = min(GT, n - i0), i1 = i0 + nb;
-        // tmp (nb x i1) = -L[I, 0:i0] Linv[0:i0, 0:i1]
-        if (i0 > 0) team_gemm(t, false, false, nb, i1, i0, -1.0, L + i0, ldl, Linv, ldi, 0.0, tmp, GT);
-        else
-            for (long long e = t.tid(); e < (long long)nb * i1; e += t.nthreads()) tmp[(e % nb) + (e / nb) * GT] = 0.0;
-        t.sync();
-        // solve L_II X = tmp + E for each column c < i1 (one thread per column)
-        for (int c = t.tid(); c < i1; c += t.nthreads()) {
-            for (int r = 0; r < nb; r++) {
-                double v = tmp[r + (long long)c * GT] + ((i0 + r) == c ? 1.0 : 0.0);
-                for (int q = 0; q < r; q++) v -= L[(i0 + r) + (long long)(i0 + q) * ldl] * tmp[q + (long long)c * GT];
-                v /= L[(i0 + r) + (long long)(i0 + r) * ldl];
-                tmp[r + (long long)c * GT] = v;
+    for (int i0 = 0; i0 < n; i0 += CB) {
+        int nb = min(CB, n - i0);
+        double* Xii = Linv + i0 + (long long)i0 * ldi;
+        if (t.rank == 0) {
+            cta_load_lower(L + i0 + (long long)i0 * ldl, ldl, nb);
+            cta_trtri(nb);
+            for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+                int r = e % nb, c = e / nb;
+                if (r >= c) Xii[r + (long long)c * ldi] = s_tri[r][c];
             }
-            for (int r = 0; r < nb; r++) Linv[(i0 + r) + (long long)c * ldi] = (c <= i0 + r) ? tmp[r + (long long)c * GT] : 0.0;
+        }
+        if (i0 > 0) {
+            team_gemm(t, false, false, nb, i0, i0, -1.0, L + i0, ldl, Linv, ldi, 0.0, tmp, CB, GEMM_B_LOWER);
+            t.sync();  // tmp and Xii complete
+            team_gemm(t, false, false, nb, i0, nb, 1.0, Xii, ldi, tmp, CB, 0.0, Linv + i0, ldi, GEMM_A_LOWER);
         }
         t.sync();
     }
@@ -297,7 +373,7 @@ __device__ void team_trinv(const Team& t, const double* L, long long ldl, double
 constexpr int NBP = 32;
 
 // ys[q] = V[r0:n, q] . v (q < c) and ys[c + q] = W[r0:n, q] . v, into shared memory
-__device__ void team_panel_dots(const Team& t, const double* V, const double* W, long long ldv, const double* v, int r0,
+__device__ __noinline__ void team_panel_dots(const Team& t, const double* V, const double* W, long long ldv, const double* v, int r0,
                                 int n, int c, double* ys, double* gpart) {
     static_assert(2 * NBP <= 64 && TEAM_THREADS == 256, "panel dots: at most 64 values, eight per warp");
     __syncthreads();
@@ -366,7 +442,7 @@ __host__ __device__ constexpr int symv_slots(int n) { return (n + 63) / 64 + 1; 
 // of block bi (slot bj) and, strictly below the diagonal, A_ic v_i to the rows of block bj
 // (slot bi, or the extra slot rt for a diagonal tile): every (slot, row) is written exactly once,
 // so summing the rt + 1 slots of a row has a fixed order. ppart[slot * n + row]; returns rt + 1.
-__device__ int team_symv_lower(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
+__device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
                                double* ppart) {
     int m = n - r0;
     int rt = (m + 63) / 64;
@@ -452,7 +528,7 @@ __device__ int team_symv_lower(const Team& t, const double* A, long long lda, in
     return rt + 1;
 }
 
-__device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
+__device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
                                      double* V, double* W, double* vbuf, double* pbuf, double* ppart, double* gred,
                                      bool cyc = false) {
     __shared__ double ys[64];
@@ -504,11 +580,12 @@ __device__ void team_tridiag_blocked(const Team& t, double* A, long long lda, in
                 V[i + c * ldv] = v;
                 if (i > r0) A[i + (long long)j * lda] = v;
             }
+            // A[r0, j] keeps alpha: the subdiagonal lives in e[j], and every thread of the team
+            // reads alpha after the norm's barrier, so nothing may overwrite it before the next one
             if (t.tid() == 0) {
                 e[j] = beta;
                 tau[j] = tj;
                 d[j] = A[j + (long long)j * lda];
-                A[r0 + (long long)j * lda] = beta;
             }
             t.sync();
             tick(9);
@@ -575,7 +652,7 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e, int
 }
 
 // all eigenvalues (ascending) by bisection, one thread per eigenvalue index
-__device__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w, double* gbuf) {
+__device__ __noinline__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w, double* gbuf) {
     // gbuf[0..2]: Gershgorin bounds and pivmin (computed by thread 0 of the team)
     if (t.tid() == 0) {
         double lo = INFINITY, hi = -INFINITY, emax = 0.0;
@@ -669,7 +746,7 @@ __device__ __forceinline__ double hash_uniform(unsigned int a, unsigned int b) {
 // against its earlier members). Vector q is written to column q of V (n x k, ldv). Work planes
 // u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved).
 // Returns (through flag) nonzero when a vector was not finite.
-__device__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
+__device__ __noinline__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
                            double* V, long long ldv, double* u0, double* u1, double* lm, unsigned char* piv, double* x,
                            int* flag) {
     double tnrm = 0.0;
@@ -769,10 +846,10 @@ __device__ void team_invit(const Team& t, const double* d, const double* e, cons
     t.sync();
 }
 
-// Z <- Q Z for Q = H_0 H_1 ... H_{n-3} kept in A (team_tridiag), Z = V (n x k, ldv), blocked by
+// Z <- Q Z for Q = H_0 H_1 ... H_{n-3} kept in A (team_tridiag_blocked), Z = V (n x k, ldv), blocked by
 // 64 reflectors (compact WY: H_b..H_{b+nb-1} = I - Vb T Vb^T, T upper triangular).
 // Work: vb (n x 64), tb (64 x 64), gm (64 x 64), y (64 x k), y2 (64 x k).
-__device__ void team_backtransform(const Team& t, const double* A, long long lda, const double* tau, int n, int k,
+__device__ __noinline__ void team_backtransform(const Team& t, const double* A, long long lda, const double* tau, int n, int k,
                                    double* V, long long ldv, double* vb, double* tb, double* gm, double* y, double* y2) {
     int nrefl = n - 2;
     if (nrefl <= 0 || k <= 0) return;

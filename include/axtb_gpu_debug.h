@@ -25,6 +25,8 @@ enum AxtbDebugQuantity {
     AXTB_DBG_WDENSITY = 9,    /* nao*nao energy-weighted density (after a gradient run) */
     AXTB_DBG_EEQ = 10,        /* nat EEQ start charges */
     AXTB_DBG_LINV = 11,       /* nao*nao inverse Cholesky factor of the overlap */
+    AXTB_DBG_EIGEN_CYCLES = 12, /* 1 value: SM clock cycles of the molecule's last eigen phase
+                                   (runs with profiling on; 0 otherwise) */
 };
 
 /* Per-kernel timing: with profiling on, every kernel launch of a run is bracketed by CUDA

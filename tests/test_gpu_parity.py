@@ -121,6 +121,21 @@ def test_deterministic(engine, golden):
     assert np.array_equal(r1.gradient, r2.gradient)
 
 
+def test_batch_deterministic(engine):
+    """Two runs of a 512-molecule mixed batch give the same bits and iteration counts: every
+    reduction of the engine has a fixed order and no step reads a value another thread may
+    still be writing (a racy mixer step counter once sent a few molecules per thousand off
+    their SCC path, costing them extra iterations)."""
+    from axtb_b200 import structures as S
+
+    b = engine.Batch(S.mixed_batch(512, seed=3), accuracy=0.1)
+    r1 = b.run(gradient=True)
+    r2 = b.run(gradient=True)
+    assert [r.iterations for r in r1] == [r.iterations for r in r2]
+    assert all(x.energy == y.energy and np.array_equal(x.gradient, y.gradient) for x, y in zip(r1, r2))
+    assert max(r.iterations for r in r1) <= 12
+
+
 def test_input_errors(engine):
     from axtb_b200 import AxtbError
 
