@@ -83,7 +83,7 @@ class _ResultBuffers:
 def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0):
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
                                 damping=float(damping), guess=0 if guess == "eeq" else 1,
-                                precision=0 if precision == "fp64" else 1, device=int(device))
+                                precision={"fp64": 0, "split": 1}[precision], device=int(device))
 
 
 class Calculator:

@@ -179,6 +179,7 @@ void check_options(const Opt& o) {
     if (!(o.etemp >= 0.0 && std::isfinite(o.etemp))) throw Fail(AXTB_ERR_INPUT, "electronic temperature must be >= 0 K");
     if (!(o.damping > 0.0 && o.damping <= 1.0)) throw Fail(AXTB_ERR_INPUT, "SCF damping must be in (0, 1]");
     if (o.max_iter <= 0) throw Fail(AXTB_ERR_INPUT, "the SCF needs at least 1 iteration");
+    if (o.precision != 0 && o.precision != 1) throw Fail(AXTB_ERR_INPUT, "precision must be 0 (FP64) or 1 (split)");
 }
 
 // ------------------------------------------------------------------ device arena
@@ -625,6 +626,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.econv = 1e-6 * o.acc;
     b.pconv = 2e-5 * o.acc;
     b.max_iter = o.max_iter;
+    b.split = o.precision == 1 ? 1 : 0;
     // state
     axg::State& s = S;
     s.xyz = ar.take<double>(natT * 3);

@@ -65,6 +65,7 @@ struct Batch {
     double damping;
     double econv, pconv;
     int max_iter;
+    int split;                        // 1: basis-transform and W GEMMs in split precision
 };
 
 // per-geometry and per-iteration device state

@@ -98,9 +98,13 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     long long t0__ = clock64(), tstart = t0__;
     // F' = L^-1 F L^-T (L^-1 is lower triangular; F' is symmetric and only its lower triangle is
     // used: the tiles on and below the diagonal are computed)
-    team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n, GEMM_A_LOWER);
+    // split precision for the basis transform only: an error there perturbs F', whose exactly
+    // orthonormal FP64 eigenvectors move the variational energy at second order; C and P stay
+    // FP64 (rounding in P would break its idempotency and enter the energy at first order)
+    const int sp = B.split ? GEMM_SPLIT : 0;
+    team_gemm(t, false, false, n, n, n, 1.0, Linv, n, S.F + mat, n, 0.0, X, n, GEMM_A_LOWER | sp);
     t.sync();
-    team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n, GEMM_B_UPPER | GEMM_LOWER_TILES);
+    team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n, GEMM_B_UPPER | GEMM_LOWER_TILES | sp);
     t.sync();
     TEAM_PHASE(0);
     double* d = S.dtri + ao0;
@@ -189,7 +193,7 @@ __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPla
         Cf[q] = Cm[q] * (S.focc[ao0 + c] * S.emo[ao0 + c]);
     }
     t.sync();
-    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.W + mat, n, GEMM_LOWER_TILES);
+    team_gemm(t, false, true, n, n, k, 1.0, Cf, n, Cm, n, 0.0, S.W + mat, n, GEMM_LOWER_TILES | (B.split ? GEMM_SPLIT : 0));
     t.sync();
     team_mirror_lower(t, S.W + mat, n, 0, n);
     t.sync();

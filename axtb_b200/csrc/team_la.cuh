@@ -14,6 +14,7 @@
 // (compact WY) back-transformation on GEMMs.
 #pragma once
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 
 #include "common.cuh"
 
@@ -113,8 +114,13 @@ __device__ double team_sum(const Team& t, double v, double* gred) {
 //   GEMM_A_LOWER  op(A) lower triangular: k <= row      GEMM_A_UPPER  op(A) upper: k >= row
 //   GEMM_B_UPPER  op(B) upper triangular: k <= col      GEMM_B_LOWER  op(B) lower: k >= col
 //   GEMM_LOWER_TILES  only tiles with bi >= bj
+// GEMM_SPLIT computes the products in split precision instead of FP64: every operand value is
+// rounded to FP32 and split into three BF16 parts (x ~ h + m + l, 24 significant bits, the
+// width of FP32), and A B ~ the six products of significance down to 2^-16 (Al Bh + Am Bm +
+// Ah Bl, then Am Bh + Ah Bm, then Ah Bh) on the BF16 tensor cores (mma.sync m16n8k16), summed in
+// FP32 within each k-step of 16 and in FP64 across k-steps; the result is stored in FP64.
 constexpr int GT = 64, GK = 16;
-enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8, GEMM_B_LOWER = 16 };
+enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8, GEMM_B_LOWER = 16, GEMM_SPLIT = 32 };
 
 // One shared-memory work area per CTA, used in turn (never at the same time, each user starting
 // and ending at a CTA barrier) by the GEMM's staging buffers and the Cholesky's diagonal block.
@@ -129,9 +135,32 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                  : "d"(a), "d"(b));
 }
 
-__device__ __noinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha, const double* A,
-                          long long lda, const double* B, long long ldb, double beta, double* Cm, long long ldc,
-                          int flags = 0) {
+// two FP64 values -> three BF16 parts each (x ~ h + m + l after rounding to FP32), packed in
+// pairs as mma operands (the first value in the low half)
+__device__ __forceinline__ void split_pair(double a, double b, unsigned& hi, unsigned& mid, unsigned& lo) {
+    float fa = (float)a, fb = (float)b;
+    __nv_bfloat162 h = __floats2bfloat162_rn(fa, fb);
+    float2 hf = __bfloat1622float2(h);
+    float ra = fa - hf.x, rb = fb - hf.y;
+    __nv_bfloat162 m = __floats2bfloat162_rn(ra, rb);
+    float2 mf = __bfloat1622float2(m);
+    __nv_bfloat162 l = __floats2bfloat162_rn(ra - mf.x, rb - mf.y);
+    hi = *reinterpret_cast<unsigned*>(&h);
+    mid = *reinterpret_cast<unsigned*>(&m);
+    lo = *reinterpret_cast<unsigned*>(&l);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float* c, const unsigned* a, const unsigned* b) {
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <bool SPLIT>
+__device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha,
+                                         const double* A, long long lda, const double* B, long long ldb, double beta,
+                                         double* Cm, long long ldc, int flags) {
     auto& As = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work);
     auto& Bs = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work + 2 * GK * (GT + 2));
     if (M <= 0 || N <= 0) return;
@@ -154,11 +183,18 @@ __device__ __noinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, i
         if (flags & GEMM_B_UPPER) ke = min(ke, col0 + GT);
         if (flags & GEMM_A_UPPER) kb = max(kb, (row0 / GK) * GK);
         if (flags & GEMM_B_LOWER) kb = max(kb, (col0 / GK) * GK);
-        double acc[4][2][2];
+        double acc[4][2][2];  // FP64: 4 x 2 tiles of 8 x 8 per warp
+        double accf[2][2][4];  // split: 2 x 2 tiles of 16 x 8 per warp (FP64 sum of FP32 k-step partials)
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
             for (int j = 0; j < 2; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int h = 0; h < 4; h++) accf[i][j][h] = 0.0;
         double ra[4], rb[4];
         auto load = [&](int k0) {
 #pragma unroll
@@ -186,17 +222,52 @@ __device__ __noinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, i
         for (int k0 = kb; k0 < ke; k0 += GK) {
             bool more = k0 + GK < ke;
             if (more) load(k0 + GK);
+            if constexpr (SPLIT) {
+                // one k16 step: A rows g, g + 8 of each 16-row tile; k = 2 lc (+1), 2 lc + 8 (+1)
+                unsigned ah[2][4], am[2][4], al[2][4], bh[2][2], bm[2][2], bl[2][2];
+                const int k0s = 2 * lc;
 #pragma unroll
-            for (int kk = 0; kk < GK; kk += 4) {
-                double af[4], bf[2];
+                for (int i = 0; i < 2; i++) {
+                    int r = wm * 32 + i * 16 + lr;
+                    split_pair(As[cur][k0s][r], As[cur][k0s + 1][r], ah[i][0], am[i][0], al[i][0]);
+                    split_pair(As[cur][k0s][r + 8], As[cur][k0s + 1][r + 8], ah[i][1], am[i][1], al[i][1]);
+                    split_pair(As[cur][k0s + 8][r], As[cur][k0s + 9][r], ah[i][2], am[i][2], al[i][2]);
+                    split_pair(As[cur][k0s + 8][r + 8], As[cur][k0s + 9][r + 8], ah[i][3], am[i][3], al[i][3]);
+                }
 #pragma unroll
-                for (int i = 0; i < 4; i++) af[i] = As[cur][kk + lc][wm * 32 + i * 8 + lr];
+                for (int j = 0; j < 2; j++) {
+                    int c = wn * 16 + j * 8 + lr;
+                    split_pair(Bs[cur][k0s][c], Bs[cur][k0s + 1][c], bh[j][0], bm[j][0], bl[j][0]);
+                    split_pair(Bs[cur][k0s + 8][c], Bs[cur][k0s + 9][c], bh[j][1], bm[j][1], bl[j][1]);
+                }
+                // per k-step partial sum in FP32, smallest terms first, added to the accumulator
 #pragma unroll
-                for (int j = 0; j < 2; j++) bf[j] = Bs[cur][kk + lc][wn * 16 + j * 8 + lr];
+                for (int i = 0; i < 2; i++)
 #pragma unroll
-                for (int i = 0; i < 4; i++)
+                    for (int j = 0; j < 2; j++) {
+                        float p[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                        mma_bf16_16816(p, al[i], bh[j]);
+                        mma_bf16_16816(p, am[i], bm[j]);
+                        mma_bf16_16816(p, ah[i], bl[j]);
+                        mma_bf16_16816(p, am[i], bh[j]);
+                        mma_bf16_16816(p, ah[i], bm[j]);
+                        mma_bf16_16816(p, ah[i], bh[j]);
 #pragma unroll
-                    for (int j = 0; j < 2; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                        for (int h = 0; h < 4; h++) accf[i][j][h] += (double)p[h];
+                    }
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < GK; kk += 4) {
+                    double af[4], bf[2];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) af[i] = As[cur][kk + lc][wm * 32 + i * 8 + lr];
+#pragma unroll
+                    for (int j = 0; j < 2; j++) bf[j] = Bs[cur][kk + lc][wn * 16 + j * 8 + lr];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 2; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                }
             }
             if (more) {
                 store(cur ^ 1);
@@ -204,22 +275,45 @@ __device__ __noinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, i
                 cur ^= 1;
             }
         }
+        if constexpr (SPLIT) {
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int gr = row0 + wm * 32 + i * 8 + lr;
-            if (gr >= M) continue;
+            for (int i = 0; i < 2; i++)
 #pragma unroll
-            for (int j = 0; j < 2; j++)
+                for (int j = 0; j < 2; j++)
 #pragma unroll
-                for (int h = 0; h < 2; h++) {
-                    int gc = col0 + wn * 16 + j * 8 + lc * 2 + h;
-                    if (gc >= N) continue;
-                    double* dst = &Cm[gr + (long long)gc * ldc];
-                    double v = alpha * acc[i][j][h];
-                    *dst = beta == 0.0 ? v : v + beta * *dst;
-                }
+                    for (int h = 0; h < 4; h++) {
+                        int gr = row0 + wm * 32 + i * 16 + lr + (h >> 1) * 8;
+                        int gc = col0 + wn * 16 + j * 8 + lc * 2 + (h & 1);
+                        if (gr >= M || gc >= N) continue;
+                        double* dst = &Cm[gr + (long long)gc * ldc];
+                        double v = alpha * accf[i][j][h];
+                        *dst = beta == 0.0 ? v : v + beta * *dst;
+                    }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                int gr = row0 + wm * 32 + i * 8 + lr;
+                if (gr >= M) continue;
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        int gc = col0 + wn * 16 + j * 8 + lc * 2 + h;
+                        if (gc >= N) continue;
+                        double* dst = &Cm[gr + (long long)gc * ldc];
+                        double v = alpha * acc[i][j][h];
+                        *dst = beta == 0.0 ? v : v + beta * *dst;
+                    }
+            }
         }
     }
+}
+
+__device__ __forceinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha,
+                                          const double* A, long long lda, const double* B, long long ldb, double beta,
+                                          double* Cm, long long ldc, int flags = 0) {
+    if (flags & GEMM_SPLIT) team_gemm_t<true>(t, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, Cm, ldc, flags);
+    else team_gemm_t<false>(t, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, Cm, ldc, flags);
 }
 
 #undef A_MM

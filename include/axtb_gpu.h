@@ -50,7 +50,11 @@ typedef struct AxtbOptions {
     int32_t max_iter;  /* iterations of the SCF; 250 */
     double damping;    /* Broyden damping, (0, 1]; 0.4 */
     int32_t guess;     /* 0: EEQ charges (default), 1: neutral atoms */
-    int32_t precision; /* 0: FP64 throughout (default); 1: split precision (3xBF16 dense products) */
+    int32_t precision; /* 0: FP64 throughout (default); 1: split precision: the basis-transform
+                          (F' = L^-1 F L^-T) and energy-weighted-density GEMMs as BF16 tensor-core
+                          products of three-part split operands (FP32-level accuracy); eigensolver,
+                          C, P, mixer and sums stay FP64. For SCC accuracy >= ~1e-3; tighter
+                          settings ask for energy changes below its rounding floor. */
     int32_t device;    /* CUDA device ordinal; 0 */
 } AxtbOptions;
 
