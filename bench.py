@@ -154,6 +154,39 @@ def measured_peaks():
 
 
 # ------------------------------------------------------------------------------ main
+# DRAM bytes (read + write) of one eigen-phase launch of the team kernel with all 4096 molecules
+# active (the first SCC iteration), from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum`
+# on this bench's default workload (summary and command: profiles/team_eigen_mixed4096_dram.md)
+TEAM_EIGEN_TRAFFIC = 334.92e9 + 76.32e9
+
+
+def large_point(device):
+    """s/point of (H2O)1000 (3000 atoms, 6000 AOs; 10x10x10 lattice rule, seed 0) through the
+    public API (host positions in, energy and gradient out), FP64 and split precision, after one
+    warm-up point each; the split run's |dE| and max |dG| against the FP64 one."""
+    import torch
+
+    from axtb_b200 import Batch, structures
+
+    z, x = structures.water_cluster(1000, seed=0, dims=(10, 10, 10))
+    res = {}
+    for prec in ("fp64", "split"):
+        b = Batch([(z, x)], accuracy=1.0, precision=prec, device=device)
+        b.run([x], gradient=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = b.run([x], gradient=True)[0]
+        torch.cuda.synchronize()
+        res[prec] = (r, time.perf_counter() - t0)
+        b.close()
+    (r64, t64), (rsp, tsp) = res["fp64"], res["split"]
+    return {"system": "(H2O)1000: 3000 atoms, 6000 AOs (10x10x10 lattice rule, seed 0), accuracy 1",
+            "s_per_point": t64, "iterations": r64.iterations, "status": r64.status, "energy": r64.energy,
+            "split": {"s_per_point": tsp, "iterations": rsp.iterations, "abs_dE": abs(rsp.energy - r64.energy),
+                      "max_abs_dG": float(np.abs(rsp.gradient - r64.gradient).max()),
+                      "speedup_vs_fp64": t64 / tsp}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -165,6 +198,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="skip the (H2O)1000 single point")
     args = ap.parse_args()
     rank, world, local = rank_info()
 
@@ -298,13 +332,23 @@ def main():
         tot_ms = sum(v["ms"] for v in kern.values())
         if kd["flops"] > 0:
             ach = kd["flops"] / (kd["ms"] / 1e3) / 1e12
+            traffic = TEAM_EIGEN_TRAFFIC if name == "team_eigen" and args.nmol == 4096 else None
             roof = {"kernel": name, "bound": "tensor", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                    "frac": ach / fp64, "traffic": None, "share": kd["ms"] / tot_ms,
-                    "note": "FP64 dense algebra; peak = measured torch float64 8192^3 GEMM on this GPU"}
+                    "frac": ach / fp64, "traffic": traffic, "share": kd["ms"] / tot_ms,
+                    "note": "FP64 dense algebra; peak = measured torch float64 8192^3 GEMM on this GPU; "
+                            "traffic = ncu DRAM bytes of the first (all-active) eigen launch"}
         else:
             ach = kd["bytes"] / (kd["ms"] / 1e3) / 1e9
             roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                     "frac": ach / peaks["hbm_gbs"], "traffic": None, "share": kd["ms"] / tot_ms}
+        # whole-step roofline: sum over kernels of max(FLOPs / FP64 peak, bytes / HBM), against the
+        # measured step (kernels without an algorithmic count contribute no roofline time)
+        t_roof = sum(max(v["flops"] / (fp64 * 1e12), v["bytes"] / (peaks["hbm_gbs"] * 1e9)) for v in kern.values())
+        step_roof = {"t_roof_ms": t_roof * 1e3 / args.steps, "t_step_ms": tmax / args.steps * 1e3,
+                     "frac": t_roof / tmax}
+        large = None
+        if not args.no_large and world == 1:
+            large = large_point(local)
         cb = None
         if not args.no_cpu:
             cb = cpu_baseline(mols, args.accuracy, budget_s=args.cpu_budget)
@@ -314,7 +358,8 @@ def main():
                "config": {"workload": WORKLOAD, "nmol": args.nmol, "atoms": natT, "accuracy": args.accuracy,
                           "l2": "flushed between timed steps (256 MB write)", "parallelism": f"molecule-sharded x{world}",
                           "failed_molecules": fails},
-               "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb,
+               "e2e": e2e, "gpu_launches": launches, "roofline": roof, "step_roofline": step_roof,
+               "large_point": large, "cpu_baseline": cb,
                "clocks": clk.summary(), "kernel_ms": {k: round(v["ms"], 3) for k, v in kern.items()}}
         print(json.dumps(out), flush=True)
     if world > 1:
