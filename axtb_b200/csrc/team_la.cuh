@@ -470,7 +470,8 @@ constexpr int NBP = 32;
 __device__ __noinline__ void team_panel_dots(const Team& t, const double* V, const double* W, long long ldv, const double* v, int r0,
                                 int n, int c, double* ys, double* gpart) {
     static_assert(2 * NBP <= 64 && TEAM_THREADS == 256, "panel dots: at most 64 values, eight per warp");
-    __syncthreads();
+    // no barrier first: warps that finish their symv items start here (ys was last read before
+    // the previous column's team sums)
     int nq = 2 * c;
     // a grid team splits the rows over PD_PARTS CTAs only (few partials to gather afterwards)
     int parts = t.global ? min(t.size, PD_PARTS) : 1;
@@ -526,37 +527,41 @@ __device__ __noinline__ void team_panel_dots(const Team& t, const double* V, con
     __syncthreads();
 }
 
-// Column-chunk slots of the symv partial sums for an n x n matrix (tiles of 64 plus one).
-__host__ __device__ constexpr int symv_slots(int n) { return (n + 63) / 64 + 1; }
+// Slots of the symv partial sums for an n x n matrix: 4 per 64-column block plus one.
+__host__ __device__ constexpr int symv_slots(int n) { return 4 * ((n + 63) / 64) + 1; }
 
 // y = A[r0:n, r0:n] v from the lower triangle only (A symmetric; the strict upper triangle is
 // never read and may hold stale values). The trailing matrix is cut into 64 x 64 tiles (blocks
-// counted from r0, bi >= bj); a warp takes a tile, each lane two of its rows (lane, lane + 32),
-// and reads 16 columns per round (32 loads in flight per lane). A tile adds A_ic v_c to the rows
-// of block bi (slot bj) and, strictly below the diagonal, A_ic v_i to the rows of block bj
-// (slot bi, or the extra slot rt for a diagonal tile): every (slot, row) is written exactly once,
-// so summing the rt + 1 slots of a row has a fixed order. ppart[slot * n + row]; returns rt + 1.
-__device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long long lda, int r0, int n, const double* v,
-                               double* ppart) {
+// counted from r0, bi >= bj) and each tile into four 16-column quarters; a warp takes a
+// (tile, quarter) item, each lane two of its rows (lane, lane + 32), 32 loads in flight per lane.
+// An item adds A_ic v_c to the rows of block bi and, strictly below the diagonal, A_ic v_i to its
+// 16 columns (rows of block bj). Slots, per row block R (rt blocks in all): the row sums of items
+// (R, bj, q) in slot 4 bj + q; the transposed sums of items (bi > R, R, q) in slot 3R + 3 + bi;
+// the diagonal tile's transposed part in slot 3R + 3 + rt. Every (slot, row) is written exactly
+// once, so the rows of block R sum their 3R + 4 + rt slots in a fixed order. ppart[slot * n + row];
+// returns rt.
+__device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long long lda, int r0, int n,
+                                            const double* v, double* ppart) {
     int m = n - r0;
     int rt = (m + 63) / 64;
-    int ntile = rt * (rt + 1) / 2;
+    int nitem = 4 * (rt * (rt + 1) / 2);
     int lane = threadIdx.x & 31;
-    for (int it = t.warp(); it < ntile; it += t.nwarps()) {
-        // it = bi (bi + 1) / 2 + bj
-        int bi = (int)((sqrt(8.0 * it + 1.0) - 1.0) * 0.5);
-        while ((bi + 1) * (bi + 2) / 2 <= it) bi++;
-        while (bi * (bi + 1) / 2 > it) bi--;
-        int bj = it - bi * (bi + 1) / 2;
+    for (int it = t.warp(); it < nitem; it += t.nwarps()) {
+        int tl = it >> 2, qt = it & 3;
+        // tl = bi (bi + 1) / 2 + bj
+        int bi = (int)((sqrt(8.0 * tl + 1.0) - 1.0) * 0.5);
+        while ((bi + 1) * (bi + 2) / 2 <= tl) bi++;
+        while (bi * (bi + 1) / 2 > tl) bi--;
+        int bj = tl - bi * (bi + 1) / 2;
         bool diag = bi == bj;
-        int i0 = r0 + bi * 64, c0 = r0 + bj * 64, c1 = min(n, c0 + 64);
+        int i0 = r0 + bi * 64, c0 = r0 + bj * 64, c1 = min(n, c0 + 64), cb = c0 + 16 * qt;
         int ia = i0 + lane, ib = ia + 32;
         bool oka = ia < n, okb = ib < n;
         int la = oka ? ia : n - 1, lb = okb ? ib : n - 1;
-        double va = oka ? v[ia] : 0.0, vb = okb ? v[ib] : 0.0;
         double ra = 0.0, rb = 0.0;
-        int tslot = diag ? rt : bi;
-        for (int cb = c0; cb < c1; cb += 16) {
+        if (cb < c1) {  // uniform over the warp
+            double va = oka ? v[ia] : 0.0, vb = okb ? v[ib] : 0.0;
+            int tslot = 3 * bj + 3 + (diag ? rt : bi);
             double xa[16], xb[16];
 #pragma unroll
             for (int u = 0; u < 16; u++) {
@@ -616,10 +621,11 @@ __device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long
             int cu = cb + ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
             if ((lane & 1) == 0 && cu < c1) ppart[(long long)tslot * n + cu] = cs;
         }
-        if (oka) ppart[(long long)bj * n + ia] = ra;
-        if (okb) ppart[(long long)bj * n + ib] = rb;
+        int rslot = 4 * bj + qt;  // written even for an empty quarter (zeros)
+        if (oka) ppart[(long long)rslot * n + ia] = ra;
+        if (okb) ppart[(long long)rslot * n + ib] = rb;
     }
-    return rt + 1;
+    return rt;
 }
 
 __device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
@@ -685,14 +691,15 @@ __device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long
             tick(9);
             // (3) w = tau (A v - W V^T v - V W^T v) - tau^2/2 (..) v
             if (tj != 0.0) {
-                int nch = team_symv_lower(t, A, lda, r0, n, vbuf, ppart);
+                int rt = team_symv_lower(t, A, lda, r0, n, vbuf, ppart);
                 tick(10);
                 team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);  // its barrier also publishes ppart
                 tick(11);
                 double pv = 0.0;
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
                     double s = 0.0;
-                    for (int ch = 0; ch < nch; ch++) s += ppart[(long long)ch * n + i];
+                    int nsl = 3 * ((i - r0) >> 6) + 4 + rt;  // this row's symv slots
+                    for (int ch = 0; ch < nsl; ch++) s += ppart[(long long)ch * n + i];
                     for (int q = 0; q < c; q++) s -= W[i + q * ldv] * ys[q] + V[i + q * ldv] * ys[c + q];
                     s *= tj;
                     pbuf[i] = s;
@@ -837,7 +844,10 @@ __device__ __forceinline__ double hash_uniform(unsigned int a, unsigned int b) {
 
 // Eigenvectors of the tridiagonal (d, e) for the eigenvalues w[0..k) by inverse iteration, one
 // thread per cluster of eigenvalues closer than ctol (vectors of a cluster re-orthogonalised
-// against its earlier members). Vector q is written to column q of V (n x k, ldv). Work planes
+// against its earlier members). Two solves per vector from a hashed start: with eigenvalues
+// from bisection to working precision the first solve already amplifies the wanted direction by
+// ~1/eps, the second one settles it (LAPACK's dstein stops at that growth and adds one solve).
+// Vector q is written to column q of V (n x k, ldv). Work planes
 // u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved).
 // Returns (through flag) nonzero when a vector was not finite.
 __device__ __noinline__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
@@ -890,7 +900,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                 u0[ix] = (ca == 0.0) ? pivmin : ca;
             }
             for (int i = 0; i < n; i++) x[(long long)i * LD + q] = hash_uniform((unsigned)q, (unsigned)i);
-            for (int iter = 0; iter < 3; iter++) {
+            for (int iter = 0; iter < 2; iter++) {
                 // forward: L with the row interchanges
                 for (int i = 0; i + 1 < n; i++) {
                     long long ix = (long long)i * LD + q, ix1 = ix + LD;
