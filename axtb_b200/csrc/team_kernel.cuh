@@ -88,6 +88,45 @@ __device__ void mol_eeq(const Team& t, const Batch& B, State& S, const TeamPlan&
     t.sync();
 }
 
+// tblite Fermi filling of both spins (warp 0 of the team's first CTA): focc = f_alpha + f_beta,
+// kocc, -TS; *more = 1 when only kc levels are true eigenvalues (kc < n) and level kc - 1 still
+// holds more than 1e-16 electrons of either spin. Ends with a team barrier.
+__device__ void mol_fermi(const Team& t, const Batch& B, State& S, int m, const double* emo, int n, double* focc,
+                          double* occb, int kc, double* more) {
+    if (t.rank == 0 && threadIdx.x < 32) {
+        double efa, efb;
+        warp_fill(B.m_nalpha[m], B.kt, emo, n, focc, &efa);
+        warp_fill(B.m_nbeta[m], B.kt, emo, n, occb, &efb);
+        int lane = threadIdx.x;
+        double pa = 0.0, pb = 0.0, ts = 0.0, flast = 0.0;
+        int kl = 0;
+        for (int i = lane; i < n; i += 32) {
+            double fa = focc[i], fb = occb[i];
+            pa += fa;
+            pb += fb;
+            if (B.kt > 0.0) ts += log(pow(fa, fa) * pow(1.0 - fa, 1.0 - fa)) + log(pow(fb, fb) * pow(1.0 - fb, 1.0 - fb));
+            if (i == kc - 1) flast = fmax(fa, fb);
+            double f = fa + fb;
+            focc[i] = f;
+            if (f > 1e-16) kl = max(kl, i + 1);
+        }
+        pa = warp_sum(pa);
+        pb = warp_sum(pb);
+        ts = warp_sum(ts);
+        for (int o = 16; o > 0; o >>= 1) {
+            kl = max(kl, __shfl_xor_sync(0xffffffffu, kl, o));
+            flast = fmax(flast, __shfl_xor_sync(0xffffffffu, flast, o));
+        }
+        if (lane == 0) {
+            S.kocc[m] = kl;
+            S.ts[m] = ts * B.kt;
+            *more = (kc < n && flast > 1e-16) ? 1.0 : 0.0;
+            if (fabs(pa - B.m_nalpha[m]) > 1e-6 || fabs(pb - B.m_nbeta[m]) > 1e-6) atomicOr(&S.status[m], ST_FERMI);
+        }
+    }
+    t.sync();
+}
+
 __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
     int n = B.m_nao[m], ao0 = B.m_ao0[m];
     long long mat = B.m_mat0[m];
@@ -122,38 +161,24 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     TEAM_PHASE(1);
     double* emo = S.emo + ao0;
-    team_bisect(t, d, e, n, emo, wk);
+    // eigenvalues: the lowest ceil(n_occ) + a margin first; the levels above get the Gershgorin
+    // bound (occupation exactly 0 at any sensible kT). If the highest computed level still holds
+    // more than 1e-16 electrons (small gap, high temperature), the rest are computed and the
+    // filling is redone, so every level with f > 1e-16 is a true eigenvalue.
+    team_gershgorin(t, d, e, n, wk);
+    int kc = min(n, (int)ceil(fmax(B.m_nalpha[m], B.m_nbeta[m])) + max(16, n / 16));
+    team_bisect(t, d, e, n, emo, wk, 0, kc);
+    for (int q = kc + t.tid(); q < n; q += t.nthreads()) emo[q] = wk[1];
+    t.sync();
     TEAM_PHASE(2);
-    // Fermi filling of both spins (warp 0 of CTA 0), kocc and -TS
     double* focc = S.focc + ao0;
     double* occb = wk + 8;  // n entries
-    if (t.rank == 0 && threadIdx.x < 32) {
-        double efa, efb;
-        warp_fill(B.m_nalpha[m], B.kt, emo, n, focc, &efa);
-        warp_fill(B.m_nbeta[m], B.kt, emo, n, occb, &efb);
-        int lane = threadIdx.x;
-        double pa = 0.0, pb = 0.0, ts = 0.0;
-        int kl = 0;
-        for (int i = lane; i < n; i += 32) {
-            double fa = focc[i], fb = occb[i];
-            pa += fa;
-            pb += fb;
-            if (B.kt > 0.0) ts += log(pow(fa, fa) * pow(1.0 - fa, 1.0 - fa)) + log(pow(fb, fb) * pow(1.0 - fb, 1.0 - fb));
-            double f = fa + fb;
-            focc[i] = f;
-            if (f > 1e-16) kl = max(kl, i + 1);
-        }
-        pa = warp_sum(pa);
-        pb = warp_sum(pb);
-        ts = warp_sum(ts);
-        for (int o = 16; o > 0; o >>= 1) kl = max(kl, __shfl_xor_sync(0xffffffffu, kl, o));
-        if (lane == 0) {
-            S.kocc[m] = kl;
-            S.ts[m] = ts * B.kt;
-            if (fabs(pa - B.m_nalpha[m]) > 1e-6 || fabs(pb - B.m_nbeta[m]) > 1e-6) atomicOr(&S.status[m], ST_FERMI);
-        }
+    mol_fermi(t, B, S, m, emo, n, focc, occb, kc, wk + 3);
+    if (wk[3] != 0.0) {
+        team_bisect(t, d, e, n, emo, wk, kc, n);
+        TEAM_PHASE(2);
+        mol_fermi(t, B, S, m, emo, n, focc, occb, n, wk + 3);
     }
-    t.sync();
     TEAM_PHASE(3);
     int k = S.kocc[m];
     double* Zm = S.Z + mat;

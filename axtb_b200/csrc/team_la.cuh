@@ -8,8 +8,8 @@
 // the reduced matrix L^-1 F L^-T, its eigenvalues and occupied eigenvectors, C = L^-T U; and
 // crates/base/src/linalg/density.rs: P = C diag(f) C^T) with B200-friendly algorithms:
 // blocked right-looking Cholesky, a row-block triangular inverse on GEMMs, Householder
-// tridiagonalisation with 2-D split symmetric matrix-vector products, Sturm-count bisection for
-// all eigenvalues (one thread per eigenvalue), inverse iteration for the occupied vectors (one
+// tridiagonalisation with lower-triangle symmetric matrix-vector products, Sturm-count bisection
+// (one thread per eigenvalue, the levels up to the Fermi level), inverse iteration for the occupied vectors (one
 // thread per vector, re-orthogonalised within clusters of close eigenvalues) and the blocked
 // (compact WY) back-transformation on GEMMs.
 #pragma once
@@ -697,9 +697,19 @@ __device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long
                 tick(11);
                 double pv = 0.0;
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
-                    double s = 0.0;
                     int nsl = 3 * ((i - r0) >> 6) + 4 + rt;  // this row's symv slots
-                    for (int ch = 0; ch < nsl; ch++) s += ppart[(long long)ch * n + i];
+                    // four independent partial sums (four loads in flight), combined in a fixed order
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    const double* pp = ppart + i;
+                    int ch = 0;
+                    for (; ch + 3 < nsl; ch += 4) {
+                        s0 += pp[(long long)ch * n];
+                        s1 += pp[(long long)(ch + 1) * n];
+                        s2 += pp[(long long)(ch + 2) * n];
+                        s3 += pp[(long long)(ch + 3) * n];
+                    }
+                    for (; ch < nsl; ch++) s0 += pp[(long long)ch * n];
+                    double s = (s0 + s1) + (s2 + s3);
                     for (int q = 0; q < c; q++) s -= W[i + q * ldv] * ys[q] + V[i + q * ldv] * ys[c + q];
                     s *= tj;
                     pbuf[i] = s;
@@ -752,9 +762,9 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e, int
     return cnt;
 }
 
-// all eigenvalues (ascending) by bisection, one thread per eigenvalue index
-__device__ __noinline__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w, double* gbuf) {
-    // gbuf[0..2]: Gershgorin bounds and pivmin (computed by thread 0 of the team)
+// Gershgorin bounds of the symmetric tridiagonal (d, e) and the pivot floor into gbuf[0..2]
+// (thread 0 of the team; the team barrier publishes them)
+__device__ void team_gershgorin(const Team& t, const double* d, const double* e, int n, double* gbuf) {
     if (t.tid() == 0) {
         double lo = INFINITY, hi = -INFINITY, emax = 0.0;
         for (int i = 0; i < n; i++) {
@@ -771,8 +781,14 @@ __device__ __noinline__ void team_bisect(const Team& t, const double* d, const d
         gbuf[2] = DBL_MIN * fmax(1.0, emax);
     }
     t.sync();
+}
+
+// eigenvalues k0..k1-1 (ascending order) by bisection, one thread per eigenvalue index; gbuf holds
+// team_gershgorin's bounds
+__device__ __noinline__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w,
+                                         const double* gbuf, int k0, int k1) {
     double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
-    for (int k = t.tid(); k < n; k += t.nthreads()) {
+    for (int k = k0 + t.tid(); k < k1; k += t.nthreads()) {
         double lo = glo, hi = ghi;
         for (int it = 0; it < 200; it++) {
             double mid = 0.5 * (lo + hi);
