@@ -157,7 +157,7 @@ def measured_peaks():
 # DRAM bytes (read + write) of one eigen-phase launch of the team kernel with all 4096 molecules
 # active (the first SCC iteration), from `ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum`
 # on this bench's default workload (summary and command: profiles/team_eigen_mixed4096_dram.md)
-TEAM_EIGEN_TRAFFIC = 334.92e9 + 76.32e9
+TEAM_EIGEN_TRAFFIC = 331.42e9 + 77.41e9
 
 
 def large_point(device):
