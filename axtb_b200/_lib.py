@@ -20,12 +20,13 @@ AXTB_ERR_NUMERICAL = 4
 AXTB_ERR_DEVICE = 5
 
 DBG = {"cn": 0, "overlap": 1, "h0": 2, "dipole": 3, "quadrupole": 4, "density": 5, "fock": 6, "emo": 7,
-       "focc": 8, "wdensity": 9, "eeq": 10, "linv": 11, "eigen_cycles": 12}
+       "focc": 8, "wdensity": 9, "eeq": 10, "linv": 11, "eigen_cycles": 12,
+       "status_bits": 13}
 
 
 class AxtbOptions(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("etemp", C.c_double), ("max_iter", C.c_int32), ("damping", C.c_double),
-                ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32)]
+                ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("mixer", C.c_int32)]
 
 
 class AxtbResult(C.Structure):
@@ -33,7 +34,7 @@ class AxtbResult(C.Structure):
                 ("dipole", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)), ("dpat", C.POINTER(C.c_double)),
                 ("qpat", C.POINTER(C.c_double)), ("terms", C.c_double * 8), ("iterations", C.c_int32),
                 ("converged", C.c_int32), ("status", C.c_int32), ("energy_change", C.c_double),
-                ("residual", C.c_double)]
+                ("residual", C.c_double), ("mixer_used", C.c_int32)]
 
 
 class AxtbMol(C.Structure):

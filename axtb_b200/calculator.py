@@ -43,6 +43,7 @@ class SinglePoint:
     status: int = 0
     energy_change: float = 0.0
     residual: float = 0.0
+    mixer_used: str = "broyden"  # "broyden", "diis" or "diis-fallback" (auto after Broyden failed)
 
 
 def _ptr(a):
@@ -77,13 +78,27 @@ class _ResultBuffers:
                            dipole=self.dip.copy(), qsh=self.qsh.copy(), dpat=self.dp.copy(), qpat=self.qp.copy(),
                            terms=dict(zip(TERM_NAMES, list(r.terms))), iterations=r.iterations,
                            converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
-                           residual=r.residual)
+                           residual=r.residual, mixer_used=MIXER_USED[r.mixer_used])
 
 
-def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0):
+# SCC mixers by name (crates/axtb/src/scf/mixing.rs:202-214: case-insensitive, "pulay" = DIIS)
+MIXERS = {"auto": 0, "broyden": 1, "diis": 2, "pulay": 2}
+MIXER_USED = ("broyden", "diis", "diis-fallback")
+
+
+def _mixer(name: str) -> int:
+    try:
+        return MIXERS[name.lower()]
+    except KeyError:
+        raise AxtbError(1, f"unknown SCF mixer {name!r} (auto, broyden or diis)") from None
+
+
+def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0,
+             mixer="auto"):
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
                                 damping=float(damping), guess=0 if guess == "eeq" else 1,
-                                precision={"fp64": 0, "split": 1}[precision], device=int(device))
+                                precision={"fp64": 0, "split": 1}[precision], device=int(device),
+                                mixer=_mixer(mixer))
 
 
 class Calculator:
@@ -208,7 +223,7 @@ class Batch:
         z, _ = self.mols[mol]
         nat = len(z)
         nsh, nao = basis_size(z)
-        size = {"cn": nat, "eeq": nat, "emo": nao, "focc": nao, "eigen_cycles": 1, "dipole": 3 * nao * nao,
+        size = {"cn": nat, "eeq": nat, "emo": nao, "focc": nao, "eigen_cycles": 1, "status_bits": 1, "dipole": 3 * nao * nao,
                 "quadrupole": 6 * nao * nao}.get(what, nao * nao)
         out = np.zeros(size)
         rc = _lib.load().axtb_gpu_batch_debug(self._b, mol, _lib.DBG[what], _ptr(out))

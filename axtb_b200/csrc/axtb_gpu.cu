@@ -172,6 +172,7 @@ void check_molecule(HostMol& m) {
 struct Opt {
     double acc = 1.0, etemp = 300.0, damping = 0.4;
     int max_iter = 250, guess = 0, precision = 0, device = 0;
+    int mixer = 0;  // 0 auto (Broyden, then DIIS from the start), 1 Broyden, 2 DIIS
 };
 
 void check_options(const Opt& o) {
@@ -180,6 +181,7 @@ void check_options(const Opt& o) {
     if (!(o.damping > 0.0 && o.damping <= 1.0)) throw Fail(AXTB_ERR_INPUT, "SCF damping must be in (0, 1]");
     if (o.max_iter <= 0) throw Fail(AXTB_ERR_INPUT, "the SCF needs at least 1 iteration");
     if (o.precision != 0 && o.precision != 1) throw Fail(AXTB_ERR_INPUT, "precision must be 0 (FP64) or 1 (split)");
+    if (o.mixer < 0 || o.mixer > 2) throw Fail(AXTB_ERR_INPUT, "unknown SCF mixer (0 auto, 1 Broyden, 2 DIIS)");
 }
 
 // ------------------------------------------------------------------ device arena
@@ -287,7 +289,18 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     m_mat0.resize(nmol);
     m_pair0.resize(nmol);
     m_vec0.resize(nmol);
-    hist_cap = std::min(o.max_iter, nmol > 16 ? 64 : 128);
+    // Broyden keeps max_iter history vectors (its memory, crates/axtb/src/xtb.rs:598) up to
+    // BROYDEN_MAX_HIST when the histories of the whole batch fit in 1 GiB, else 64 (a molecule
+    // that needs more ends its Broyden attempt there); the span of each molecule also holds the
+    // DIIS history
+    {
+        long long vec = 0;
+        for (auto& h : mols) vec += h.nsh + 9LL * h.nat;
+        int full = std::min(o.max_iter, axg::BROYDEN_MAX_HIST);
+        double bytes = 16.0 * full * (double)vec + 16.0 * nmol * (double)full * full;  // df, u; a and beta
+        hist_cap = bytes <= (double)(1LL << 30) ? full : std::min(o.max_iter, 64);
+    }
+    const int hist_span = std::max(hist_cap, axg::DIIS_SLOTS);
     natT = nshT = naoT = 0;
     nnT = npairT = npdT = nvecT = nsqT = ntiles = nwk = nhist = 0;
     for (int m = 0; m < nmol; m++) {
@@ -318,7 +331,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         npairT += (long long)h.nat * (h.nat - 1) / 2;
         npdT += (long long)h.nat * (h.nat + 1) / 2;
         nvecT += m_dim[m];
-        nhist += (long long)hist_cap * m_dim[m];
+        nhist += (long long)hist_span * m_dim[m];
         nsqT += (long long)h.nat * h.nat;
         long long nt = (n + 31) / 32;
         ntiles += nt * nt;
@@ -511,6 +524,10 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     bytes += padded<unsigned char>((size_t)nnT);
     addD((size_t)naoT * 5);
     addI(nmol * 7);
+    addI(nmol);
+    addI(nmol);
+    addD((size_t)nmol * 8);                          // DIIS scalars
+    addD((size_t)nshT + (size_t)natT * 10);          // start moments
     addD((size_t)nshT * 3 + (size_t)natT * 2 + (size_t)natT * 6 + (size_t)natT * 12 + (size_t)nshT + natT * 10);
     addD((size_t)natT * 14);
     addD((size_t)naoT * 11);
@@ -663,6 +680,10 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.active = ar.take<int>(nmol);
     s.niter = ar.take<int>(nmol);
     s.iter = ar.take<int>(nmol);
+    s.mix_used = ar.take<int>(nmol);
+    s.niter_prev = ar.take<int>(nmol);
+    s.diis = ar.take<double>((size_t)nmol * 8);
+    s.start = ar.take<double>((size_t)nshT + (size_t)natT * 10);
     s.qsh_in = ar.take<double>(nshT);
     s.qsh_out = ar.take<double>(nshT);
     s.vsh = ar.take<double>(nshT);
@@ -737,9 +758,36 @@ __global__ void k_mol_sum(Batch B, const double* src, double* dst) {
     if (threadIdx.x == 0) dst[m] = s;
 }
 
+// the first attempt of molecule m starts here: counters, the mixer of the attempt (0 Broyden,
+// 1 DIIS) and a copy of the start moments for a later attempt from the same start
+__device__ void begin_attempts(const Batch& B, const State& S, int m, int mixer) {
+    int a0 = B.m_at0[m], nat = B.m_nat[m], s0 = B.m_sh0[m], nsh = B.m_nsh[m];
+    double* st_sh = S.start;
+    double* st_at = S.start + B.nshT;
+    for (int s = s0 + threadIdx.x; s < s0 + nsh; s += blockDim.x) st_sh[s] = S.qsh_in[s];
+    for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
+        double* t = st_at + 10LL * a;
+        t[0] = S.qat_in[a];
+        for (int k = 0; k < 3; k++) t[1 + k] = S.dp_in[3 * a + k];
+        for (int k = 0; k < 6; k++) t[4 + k] = S.qp_in[6 * a + k];
+    }
+    __syncthreads();
+    pack_moment(B, m, S.qsh_in, S.dp_in, S.qp_in, S.q_in + B.m_vec0[m], threadIdx.x, blockDim.x);
+    if (threadIdx.x == 0) {
+        S.elast[m] = 0.0;
+        S.iter[m] = 0;
+        S.niter[m] = 0;
+        S.niter_prev[m] = 0;
+        S.conv[m] = 0;
+        S.mix_used[m] = mixer == 2 ? 1 : 0;
+        diis_reset(B, S, m);
+        S.active[m] = S.status[m] == 0 ? 1 : 0;
+    }
+}
+
 // start moments: EEQ charges split over the shells by reference occupation
 // (crates/axtb/src/xtb.rs:522-549), zero multipoles, packed SCC vector
-__global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq) {
+__global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq, int mixer) {
     int m = blockIdx.x;
     if (m >= B.nmol) return;
     int a0 = B.m_at0[m], nat = B.m_nat[m];
@@ -757,18 +805,11 @@ __global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq) {
         for (int k = 0; k < 6; k++) S.qp_in[6 * a + k] = 0.0;
     }
     __syncthreads();
-    pack_moment(B, m, S.qsh_in, S.dp_in, S.qp_in, S.q_in + B.m_vec0[m], threadIdx.x, blockDim.x);
-    if (threadIdx.x == 0) {
-        S.elast[m] = 0.0;
-        S.iter[m] = 0;
-        S.niter[m] = 0;
-        S.conv[m] = 0;
-        S.active[m] = S.status[m] == 0 ? 1 : 0;
-    }
+    begin_attempts(B, S, m, mixer);
 }
 
 // start of a warm SCF: the previous converged output moments of every molecule
-__global__ void k_start_warm(Batch B, State S) {
+__global__ void k_start_warm(Batch B, State S, int mixer) {
     int m = blockIdx.x;
     if (m >= B.nmol) return;
     int a0 = B.m_at0[m], nat = B.m_nat[m], s0 = B.m_sh0[m], nsh = B.m_nsh[m];
@@ -779,13 +820,50 @@ __global__ void k_start_warm(Batch B, State S) {
         for (int k = 0; k < 6; k++) S.qp_in[6 * a + k] = S.qp_out[6 * a + k];
     }
     __syncthreads();
+    begin_attempts(B, S, m, mixer);
+}
+
+// the DIIS attempt of the auto plan (crates/axtb/src/xtb.rs:590-645): a molecule whose Broyden
+// attempt ended unconverged, with a failed mixer or a lost Fermi level starts again from its
+// start moments with DIIS; one that ended with an error axtb raises at once does not. Within an
+// iteration axtb checks the Fock matrix (non-finite: error), then the Fermi level (lost: next
+// attempt, crates/axtb/src/xtb.rs:1013-1025), then the energy (non-finite: error); the eigen
+// phase here goes on after a lost Fermi level, so bits it sets after one do not count. The
+// iterations of the Broyden attempt are kept for the failure report.
+__global__ void k_restart_diis(Batch B, State S) {
+    int m = blockIdx.x;
+    if (m >= B.nmol) return;
+    __shared__ int s_go;
+    if (threadIdx.x == 0) {
+        int st = S.status[m];
+        bool hard = (st & (ST_NOT_PD | ST_FOCK | ST_TIMEOUT)) != 0 ||
+                    (!(st & ST_FERMI) && (st & (ST_NONFINITE | ST_INVIT)) != 0);
+        s_go = !S.conv[m] && !hard;
+    }
+    __syncthreads();
+    if (!s_go) return;
+    int a0 = B.m_at0[m], nat = B.m_nat[m], s0 = B.m_sh0[m], nsh = B.m_nsh[m];
+    const double* st_sh = S.start;
+    const double* st_at = S.start + B.nshT;
+    for (int s = s0 + threadIdx.x; s < s0 + nsh; s += blockDim.x) S.qsh_in[s] = st_sh[s];
+    for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
+        const double* t = st_at + 10LL * a;
+        S.qat_in[a] = t[0];
+        for (int k = 0; k < 3; k++) S.dp_in[3 * a + k] = t[1 + k];
+        for (int k = 0; k < 6; k++) S.qp_in[6 * a + k] = t[4 + k];
+    }
+    __syncthreads();
     pack_moment(B, m, S.qsh_in, S.dp_in, S.qp_in, S.q_in + B.m_vec0[m], threadIdx.x, blockDim.x);
     if (threadIdx.x == 0) {
+        S.niter_prev[m] = S.niter[m];
         S.elast[m] = 0.0;
         S.iter[m] = 0;
         S.niter[m] = 0;
         S.conv[m] = 0;
-        S.active[m] = S.status[m] == 0 ? 1 : 0;
+        S.status[m] = 0;
+        S.mix_used[m] = 2;
+        diis_reset(B, S, m);
+        S.active[m] = 1;
     }
 }
 
@@ -925,7 +1003,7 @@ void AxtbBatch::run(bool want_grad, bool warm) {
            CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     bool eeq = opt.guess == 0 && !warm;
     if (warm) {
-        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S));
+        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, opt.mixer));
     } else if (eeq) {
         LAUNCH("eeq_matrix", 0, 0, k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT));
         ph = PH_EEQ;
@@ -933,25 +1011,37 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
         LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     }
-    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0));
-    // SCF
-    for (int it = 1; it <= opt.max_iter; it++) {
-        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0));
-        LAUNCH("potentials", 0, 0, k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
-        LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
-        ph = PH_EIGEN;
-        LAUNCH("team_eigen", eig_flops(act), 0,
-               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
-        LAUNCH("mulliken", 0, mat_bytes(act, 12.0),
-               k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S));
-        LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
-        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2));
-        LAUNCH("energy", 0, 0, k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
-        LAUNCH("broyden", 0, 0, k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap));
+    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, opt.mixer));
+    // SCF: the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199): Broyden, then
+    // for the molecules it left unconverged DIIS from the same start (auto); or one mixer alone
+    auto scf_attempt = [&](bool diis) {
+        for (int it = 1; it <= opt.max_iter; it++) {
+            LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0));
+            LAUNCH("potentials", 0, 0, k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+            LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
+            ph = PH_EIGEN;
+            LAUNCH("team_eigen", eig_flops(act), 0,
+                   CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+            LAUNCH("mulliken", 0, mat_bytes(act, 12.0),
+                   k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S));
+            LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
+            LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2));
+            LAUNCH("energy", 0, 0, k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+            if (diis) LAUNCH("diis", 0, 0, k_diis<<<nmol, T, 0, st>>>(B, S));
+            else LAUNCH("broyden", 0, 0, k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap));
+            CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::copy(h_act, h_act + nmol, act.begin());
+            if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
+        }
+    };
+    scf_attempt(opt.mixer == 2);
+    if (opt.mixer == 0) {
+        LAUNCH("restart_diis", 0, 0, k_restart_diis<<<nmol, T, 0, st>>>(B, S));
         CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         std::copy(h_act, h_act + nmol, act.begin());
-        if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
+        if (std::any_of(act.begin(), act.end(), [](int v) { return v != 0; })) scf_attempt(true);
     }
     if (want_grad) {
         ph = PH_WDENS;

@@ -18,7 +18,7 @@ static int status_code(int bits, int conv) {
 
 void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     vector<double> eel(nmol), erep(nmol), eatm(nmol), terms((size_t)nmol * 8), de(nmol), res(nmol);
-    vector<int> st_(nmol), conv(nmol), nit(nmol);
+    vector<int> st_(nmol), conv(nmol), nit(nmol), nit0(nmol), used(nmol);
     vector<double> grad((size_t)natT * 3), qat(natT), dp((size_t)natT * 3), qp((size_t)natT * 6), qsh(nshT);
     CK(cudaMemcpyAsync(eel.data(), S.energy, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(erep.data(), S.e_fixed, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
@@ -29,13 +29,15 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     CK(cudaMemcpyAsync(st_.data(), S.status, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(conv.data(), S.conv, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(nit.data(), S.niter, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nit0.data(), S.niter_prev, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(used.data(), S.mix_used, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(qat.data(), S.qat_out, sizeof(double) * natT, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(dp.data(), S.dp_out, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(qp.data(), S.qp_out, sizeof(double) * natT * 6, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(qsh.data(), S.qsh_out, sizeof(double) * nshT, cudaMemcpyDeviceToHost, st));
     if (want_grad) CK(cudaMemcpyAsync(grad.data(), S.grad, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    d2h_bytes += (long long)(sizeof(double) * (nmol * 14 + (size_t)natT * 10 + nshT) + sizeof(int) * nmol * 3) +
+    d2h_bytes += (long long)(sizeof(double) * (nmol * 14 + (size_t)natT * 10 + nshT) + sizeof(int) * nmol * 5) +
                  (want_grad ? (long long)sizeof(double) * natT * 3 : 0);
     for (int m = 0; m < nmol; m++) {
         AxtbResult& r = outs[m];
@@ -44,8 +46,11 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
         for (int k = 0; k < 8; k++) r.terms[k] = terms[(size_t)m * 8 + k];
         r.terms[0] = erep[m];
         r.terms[1] += eatm[m];
-        r.iterations = nit[m];
+        // iterations of the converged attempt; of both attempts when none converged
+        // (crates/axtb/src/xtb.rs:624-645)
+        r.iterations = conv[m] ? nit[m] : nit[m] + nit0[m];
         r.converged = conv[m];
+        r.mixer_used = used[m];
         r.energy_change = de[m];
         r.residual = res[m];
         r.status = status_code(st_[m], conv[m]);
@@ -85,6 +90,7 @@ static Opt to_opt(const AxtbOptions* o) {
         r.guess = o->guess;
         r.precision = o->precision;
         r.device = o->device;
+        r.mixer = o->mixer;
     }
     return r;
 }
@@ -128,6 +134,7 @@ void axtb_gpu_default_options(AxtbOptions* o) {
     o->guess = 0;
     o->precision = 0;
     o->device = 0;
+    o->mixer = 0;
 }
 
 int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao) {
@@ -392,6 +399,13 @@ int axtb_gpu_batch_debug(AxtbBatch* b, int32_t mol, int32_t what, double* out) {
             case AXTB_DBG_EEQ: cp(b->P.eeq_q + a0, nat); break;
             case AXTB_DBG_LINV: cp(b->S.Linv + mat, n2); break;
             case AXTB_DBG_EIGEN_CYCLES: cp(b->S.mol_cyc + mol, 1); break;
+            case AXTB_DBG_STATUS_BITS: {
+                int bits = 0;
+                CK(cudaMemcpyAsync(&bits, b->S.status + mol, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+                CK(cudaStreamSynchronize(b->st));
+                *out = (double)bits;
+                break;
+            }
             default: throw Fail(AXTB_ERR_INPUT, "unknown debug quantity");
         }
         CK(cudaStreamSynchronize(b->st));

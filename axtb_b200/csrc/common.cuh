@@ -19,12 +19,13 @@ constexpr int NFREQ = 23;
 // Status bits of one molecule (per-molecule word on the device)
 enum : int {
     ST_NOT_PD = 1,         // overlap (or EEQ) matrix not positive definite
-    ST_NONFINITE = 2,      // non-finite Fock matrix or energy
+    ST_NONFINITE = 2,      // non-finite energy
     ST_FERMI = 4,          // electrons not placed by the Fermi search
-    ST_MIXER = 8,          // Broyden system singular
+    ST_MIXER = 8,          // mixer failed (Broyden system singular, non-finite DIIS residual)
     ST_INVIT = 16,         // inverse iteration produced a non-finite vector
     ST_HISTORY = 32,       // Broyden history capacity exhausted
     ST_TIMEOUT = 64,       // a bounded device wait gave up
+    ST_FOCK = 128,         // non-finite Fock matrix
 };
 
 struct Batch {
@@ -33,7 +34,7 @@ struct Batch {
     long long npairT;   // sum of nat(nat-1)/2
     long long nvecT;    // sum of SCC vector lengths
     int nsp;            // distinct elements in the batch (D4 tables)
-    int hist_cap;       // Broyden history slots per molecule
+    int hist_cap;       // Broyden history slots per molecule (the span holds at least DIIS's)
     // molecules
     const int *m_nat, *m_nsh, *m_nao, *m_at0, *m_sh0, *m_ao0, *m_dim;
     const long long *m_mat0, *m_vec0, *m_pair0, *m_hist0;
@@ -91,6 +92,10 @@ struct State {
     // mixer
     double *q_in, *dq, *qlast, *dqlast, *df, *u, *amat, *omega;  // vecs; df/u: hist x vec
     int* iter;                      // nmol: mixer iteration counter
+    double* diis;                   // nmol*8: DIIS scalars
+    double* start;                  // nshT + 10 natT: start moments (qsh; qat, dp, qp per atom)
+    int* mix_used;                  // nmol: 0 Broyden, 1 DIIS, 2 DIIS after Broyden
+    int* niter_prev;                // nmol: iterations of an earlier attempt
     // per molecule scalars
     double *energy, *elast, *de, *res, *ts, *e_fixed;  // nmol
     double* terms;     // nmol*8

@@ -1,7 +1,8 @@
 // Kernels of one SCF iteration over a batch (inactive molecules skip their work):
 // potentials of the input moments (ES2, ES3, AES2, self-consistent D4), the Fock matrix,
 // Mulliken moments of the new density with the band energy, the energy of the output moments,
-// and modified Broyden mixing with the convergence test. Then the pair terms of the gradient.
+// and the convergence test with the next input by modified Broyden or DIIS mixing. Then the
+// pair terms of the gradient.
 #pragma once
 #include "common.cuh"
 #include "k_geometry.cuh"
@@ -132,7 +133,7 @@ __global__ void k_fock(Batch B, State S, const long long* m_tile0, long long nti
         if (row >= n || col >= n) continue;
         long long e = mat + row + (long long)col * n;
         double f = S.H0[e] - 0.5 * (bterm(B, S, e, ao0 + col) + bt[tx][b]);
-        if (!isfinite(f)) atomicOr(&S.status[m], ST_NONFINITE);
+        if (!isfinite(f)) atomicOr(&S.status[m], ST_FOCK);
         S.F[e] = f;
     }
 }
@@ -283,24 +284,16 @@ __device__ __forceinline__ void pack_moment(const Batch& B, int m, const double*
     }
 }
 
-// energy assembly, residual, convergence test (crates/axtb/src/scf/convergence.rs:99-130) and
-// the next input by modified Broyden mixing (crates/axtb/src/scf/mixing.rs:251-338 with
-// crates/base/src/linalg/lu.rs:81-112); one CTA per molecule
-__global__ void k_broyden(Batch B, State S, int hist_cap) {
-    int m = blockIdx.x;
-    if (m >= B.nmol || !mol_active(S, m)) return;
+// energy assembly, residual and convergence test of one SCF iteration
+// (crates/axtb/src/scf/convergence.rs:99-130, crates/axtb/src/scf/driver.rs:263-290) for the CTA
+// of molecule m; true when the molecule's SCF attempt ends here (converged, failed or out of
+// iterations) and no mixing step follows
+__device__ bool scf_iteration_end(const Batch& B, const State& S, int m) {
     int tid = threadIdx.x, nthr = blockDim.x;
     int dim = B.m_dim[m], nat = B.m_nat[m], a0 = B.m_at0[m];
     long long v0 = B.m_vec0[m];
     double* q_in = S.q_in + v0;
     double* dq = S.dq + v0;
-    double* qlast = S.qlast + v0;
-    double* dqlast = S.dqlast + v0;
-    long long h0 = B.m_hist0[m];
-    double* df = S.df + h0 * 1;  // hist_cap * dim
-    double* u = S.u + h0 * 1;
-    double* amat = S.amat + (long long)m * hist_cap * hist_cap;
-    double* omega = S.omega + (long long)m * hist_cap;
     // energy and terms (sums in atom order per thread stripe, reduced deterministically)
     double e = 0.0, t2 = 0.0, t3 = 0.0, ta = 0.0, td = 0.0, tb = 0.0;
     for (int a = tid; a < nat; a += nthr) {
@@ -326,7 +319,7 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
         rr += dq[i] * dq[i];
     }
     rr = cta_sum(rr);
-    __shared__ int s_done, s_ok;
+    __shared__ int s_done;
     if (tid == 0) {
         double res = sqrt(rr / dim);
         double de = e - S.elast[m];
@@ -359,8 +352,60 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
         }
     }
     __syncthreads();
-    if (s_done) return;
-    // ---- Broyden step (one thread advances the step counter; every thread reads it back)
+    return s_done != 0;
+}
+
+// the new input q_in into the input moments (and re-packed, as the reference packs the state it
+// unpacked: crates/axtb/src/scf/driver.rs:225-229)
+__device__ void unpack_input(const Batch& B, const State& S, int m) {
+    int tid = threadIdx.x, nthr = blockDim.x;
+    int dim = B.m_dim[m], nat = B.m_nat[m], a0 = B.m_at0[m];
+    double* q_in = S.q_in + B.m_vec0[m];
+    __syncthreads();
+    int nsh = B.m_nsh[m], s0 = B.m_sh0[m];
+    for (int i = tid; i < dim; i += nthr) {
+        double x = q_in[i];
+        if (i < nsh) S.qsh_in[s0 + i] = x;
+        else if (i < nsh + 3 * nat) S.dp_in[3 * a0 + (i - nsh)] = x;
+        else {
+            int r = i - nsh - 3 * nat, c = r % 6;
+            double y = x / (QOFF[c] ? SQRT2 : 1.0);
+            S.qp_in[6 * a0 + r] = y;
+            q_in[i] = y * (QOFF[c] ? SQRT2 : 1.0);
+        }
+    }
+    __syncthreads();
+    for (int a = tid; a < nat; a += nthr) {
+        double q = 0.0;
+        for (int s = B.a_sh0[a0 + a]; s < B.a_sh0[a0 + a] + B.a_nsh[a0 + a]; s++) q += S.qsh_in[s];
+        S.qat_in[a0 + a] = q;
+    }
+}
+
+constexpr int BROYDEN_MAX_HIST = 256;  // history slots a molecule can hold (shared solve vector)
+
+// the iteration's end and the next input by modified Broyden mixing
+// (crates/axtb/src/scf/mixing.rs:251-338 with crates/base/src/linalg/lu.rs:81-112); one CTA per
+// molecule. The Gauss elimination updates the rows below the pivot in parallel, each row with
+// the reference's operations in its order.
+__global__ void k_broyden(Batch B, State S, int hist_cap) {
+    int m = blockIdx.x;
+    if (m >= B.nmol || !mol_active(S, m)) return;
+    if (scf_iteration_end(B, S, m)) return;
+    int tid = threadIdx.x, nthr = blockDim.x;
+    int dim = B.m_dim[m];
+    long long v0 = B.m_vec0[m];
+    double* q_in = S.q_in + v0;
+    double* dq = S.dq + v0;
+    double* qlast = S.qlast + v0;
+    double* dqlast = S.dqlast + v0;
+    long long h0 = B.m_hist0[m];
+    double* df = S.df + h0;  // hist_cap * dim
+    double* u = S.u + h0;
+    double* amat = S.amat + (long long)m * hist_cap * hist_cap;
+    double* omega = S.omega + (long long)m * hist_cap;
+    __shared__ int s_ok;
+    // one thread advances the step counter; every thread reads it back
     __shared__ int s_iter;
     if (tid == 0) s_iter = ++S.iter[m];
     __syncthreads();
@@ -402,7 +447,8 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
         for (int i = tid; i < dim; i += nthr) dfi[i] *= inv;
         __syncthreads();
         // a[it1][j] = df_it1 . df_j (j <= it1), c[j] = omega_j df_j . dq
-        __shared__ double cvec[128];
+        __shared__ double cvec[BROYDEN_MAX_HIST];
+        __shared__ int s_piv;
         for (int j = 0; j < nh; j++) {
             double* dfj = df + (long long)j * dim;
             double s1 = 0.0, s2 = 0.0;
@@ -419,48 +465,62 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
             }
         }
         __syncthreads();
+        // beta (kept in the tail of amat's slab) = omega_i omega_j a_ij + omega0^2 delta_ij
+        double* bt = S.amat + (long long)B.nmol * hist_cap * hist_cap + (long long)m * hist_cap * hist_cap;
+        for (int e = tid; e < nh * nh; e += nthr) {
+            int i = e / nh, j = e % nh;
+            double v = omega[i] * omega[j] * amat[i * hist_cap + j];
+            if (i == j) v += OMEGA0 * OMEGA0;
+            bt[i * hist_cap + j] = v;
+        }
+        __syncthreads();
         if (tid == 0) {
             s_ok = 1;
-            // Gauss elimination with the last largest pivot on beta (kept in the tail of amat's slab)
-            double* bt = S.amat + (long long)B.nmol * hist_cap * hist_cap + (long long)m * hist_cap * hist_cap;
-            for (int i = 0; i < nh; i++) {
-                cvec[i] *= omega[i];
-                for (int j = 0; j < nh; j++) bt[i * hist_cap + j] = omega[i] * omega[j] * amat[i * hist_cap + j];
-                bt[i * hist_cap + i] += OMEGA0 * OMEGA0;
-            }
-            for (int col = 0; col < nh && s_ok; col++) {
+            for (int i = 0; i < nh; i++) cvec[i] *= omega[i];
+        }
+        // Gauss elimination with the last largest pivot
+        for (int col = 0; col < nh; col++) {
+            __syncthreads();
+            if (tid == 0) {
                 int piv = col;
                 for (int i = col + 1; i < nh; i++)
                     if (fabs(bt[i * hist_cap + col]) >= fabs(bt[piv * hist_cap + col])) piv = i;
-                if (bt[piv * hist_cap + col] == 0.0) {
-                    s_ok = 0;
-                    break;
+                if (bt[piv * hist_cap + col] == 0.0) s_ok = 0;
+                s_piv = piv;
+            }
+            __syncthreads();
+            if (!s_ok) break;
+            int piv = s_piv;
+            if (piv != col) {
+                for (int k = tid; k < nh; k += nthr) {
+                    double tmp = bt[col * hist_cap + k];
+                    bt[col * hist_cap + k] = bt[piv * hist_cap + k];
+                    bt[piv * hist_cap + k] = tmp;
                 }
-                if (piv != col) {
-                    for (int k = 0; k < nh; k++) {
-                        double tmp = bt[col * hist_cap + k];
-                        bt[col * hist_cap + k] = bt[piv * hist_cap + k];
-                        bt[piv * hist_cap + k] = tmp;
-                    }
+                if (tid == 0) {
                     double tmp = cvec[col];
                     cvec[col] = cvec[piv];
                     cvec[piv] = tmp;
                 }
-                for (int row = col + 1; row < nh; row++) {
-                    double f = bt[row * hist_cap + col] / bt[col * hist_cap + col];
-                    if (f != 0.0) {
-                        for (int k = col; k < nh; k++) bt[row * hist_cap + k] -= f * bt[col * hist_cap + k];
-                        cvec[row] -= f * cvec[col];
-                    }
+                __syncthreads();
+            }
+            const double* prow = bt + (long long)col * hist_cap;
+            for (int row = col + 1 + tid; row < nh; row += nthr) {
+                double* rrow = bt + (long long)row * hist_cap;
+                double f = rrow[col] / prow[col];
+                if (f != 0.0) {
+                    for (int k = col; k < nh; k++) rrow[k] -= f * prow[k];
+                    cvec[row] -= f * cvec[col];
                 }
             }
-            if (s_ok)
-                for (int col = nh - 1; col >= 0; col--) {
-                    double s = cvec[col];
-                    for (int k = col + 1; k < nh; k++) s -= bt[col * hist_cap + k] * cvec[k];
-                    cvec[col] = s / bt[col * hist_cap + col];
-                }
         }
+        __syncthreads();
+        if (tid == 0 && s_ok)
+            for (int col = nh - 1; col >= 0; col--) {
+                double s = cvec[col];
+                for (int k = col + 1; k < nh; k++) s -= bt[col * hist_cap + k] * cvec[k];
+                cvec[col] = s / bt[col * hist_cap + col];
+            }
         __syncthreads();
         if (!s_ok) {
             if (tid == 0) {
@@ -479,26 +539,176 @@ __global__ void k_broyden(Batch B, State S, int hist_cap) {
             q_in[i] = v;
         }
     }
+    unpack_input(B, S, m);
+}
+
+// ----------------------------------------------------------------------------- DIIS
+// Pulay (DIIS, Anderson) mixing with restarts (crates/axtb/src/scf/mixing.rs:342-525). Per
+// molecule, in its mixer history span (DIIS_SLOTS vectors in df and in u):
+//   df slots [0, DIIS_SIZE): inputs q_i (a ring), [DIIS_SIZE, 2 DIIS_SIZE - 1): the orthonormal
+//   basis of the residual differences, then the best input and its residual;
+//   u slots [0, DIIS_SIZE): residuals r_i (the same ring).
+// Scalars in S.diis[8 m ..]: damping, best residual norm, best seen (0/1), iterations since the
+// best, history length, ring head.
+constexpr int DIIS_SIZE = 30;
+constexpr int DIIS_SLOTS = 2 * DIIS_SIZE + 1;
+constexpr double DIIS_DEPENDENCE = 1e-2;
+constexpr int DIIS_STALL = 12;
+constexpr double DIIS_RESTART_GROWTH = 1e3, DIIS_RESTART_FLOOR = 0.1;
+
+__device__ __forceinline__ void diis_reset(const Batch& B, const State& S, int m) {
+    double* d = S.diis + 8 * m;
+    d[0] = B.damping;
+    for (int k = 1; k < 8; k++) d[k] = 0.0;
+}
+
+// the iteration's end and the next input by DIIS: the coefficients c minimise |sum c_i r_i|
+// with sum c_i = 1, from the differences r_n - r_j orthonormalised newest first by modified
+// Gram-Schmidt (a difference keeping less than DIIS_DEPENDENCE of its norm ends the basis) and
+// R g = Q^T r_n; the next input is sum c_i (q_i + damp r_i). A residual DIIS_RESTART_GROWTH times
+// the best (above DIIS_RESTART_FLOOR), or DIIS_STALL iterations without a better one, restart
+// from the best input with half the damping. One CTA per molecule.
+__global__ void k_diis(Batch B, State S) {
+    int m = blockIdx.x;
+    if (m >= B.nmol || !mol_active(S, m)) return;
+    if (scf_iteration_end(B, S, m)) return;
+    int tid = threadIdx.x, nthr = blockDim.x;
+    int dim = B.m_dim[m];
+    long long v0 = B.m_vec0[m];
+    double* q_in = S.q_in + v0;
+    const double* dq = S.dq + v0;
+    long long h0 = B.m_hist0[m];
+    double* hq = S.df + h0;                                   // input ring
+    double* hr = S.u + h0;                                    // residual ring
+    double* basis = S.df + h0 + (long long)DIIS_SIZE * dim;  // DIIS_SIZE - 1 basis vectors
+    double* best_q = S.df + h0 + (long long)(2 * DIIS_SIZE - 1) * dim;
+    double* best_r = best_q + dim;
+    double* sc = S.diis + 8 * m;
+    __shared__ double s_R[DIIS_SIZE][DIIS_SIZE];  // s_R[l][p]: entry l of column p of R
+    __shared__ double s_c[DIIS_SIZE], s_g[DIIS_SIZE];
+    __shared__ int s_kept[DIIS_SIZE];
+    double nn = 0.0;
+    for (int i = tid; i < dim; i += nthr) nn += dq[i] * dq[i];
+    double norm = sqrt(cta_sum(nn));
+    double damp = sc[0];
+    bool have_best = sc[2] != 0.0;
+    int since_best = (int)sc[3], count = (int)sc[4], head = (int)sc[5];
+    int mode = 0;  // 0 mix, 1 restart, 2 failed (the same on every thread)
+    if (!isfinite(norm)) mode = 2;
+    else if (have_best && ((norm > DIIS_RESTART_GROWTH * sc[1] && norm > DIIS_RESTART_FLOOR) ||
+                           since_best >= DIIS_STALL))
+        mode = 1;
     __syncthreads();
-    // unpack the new input (and re-pack it, as the reference packs its unpacked state)
-    int nsh = B.m_nsh[m], s0 = B.m_sh0[m];
+    if (mode == 2) {
+        if (tid == 0) {
+            S.status[m] |= ST_MIXER;
+            S.active[m] = 0;
+        }
+        return;
+    }
+    if (mode == 1) {
+        // drop the history and restart from the best input with half the damping
+        damp *= 0.5;
+        for (int i = tid; i < dim; i += nthr) q_in[i] = best_q[i] + damp * best_r[i];
+        if (tid == 0) {
+            sc[0] = damp;
+            sc[3] = 0.0;
+            sc[4] = 0.0;
+            sc[5] = 0.0;
+        }
+        unpack_input(B, S, m);
+        return;
+    }
+    bool better = !have_best || norm < sc[1];
+    if (better)
+        for (int i = tid; i < dim; i += nthr) {
+            best_q[i] = q_in[i];
+            best_r[i] = dq[i];
+        }
+    since_best = better ? 0 : since_best + 1;
+    // push (q_in, dq), dropping the oldest pair of a full history
+    if (count == DIIS_SIZE) {
+        head = (head + 1) % DIIS_SIZE;
+        count--;
+    }
+    int slot = (head + count) % DIIS_SIZE;
+    count++;
     for (int i = tid; i < dim; i += nthr) {
-        double x = q_in[i];
-        if (i < nsh) S.qsh_in[s0 + i] = x;
-        else if (i < nsh + 3 * nat) S.dp_in[3 * a0 + (i - nsh)] = x;
-        else {
-            int r = i - nsh - 3 * nat, c = r % 6;
-            double y = x / (QOFF[c] ? SQRT2 : 1.0);
-            S.qp_in[6 * a0 + r] = y;
-            q_in[i] = y * (QOFF[c] ? SQRT2 : 1.0);
+        hq[(long long)slot * dim + i] = q_in[i];
+        hr[(long long)slot * dim + i] = dq[i];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (better) sc[1] = norm;
+        sc[2] = 1.0;
+        sc[3] = since_best;
+        sc[4] = count;
+        sc[5] = head;
+    }
+    auto phys = [&](int i) { return (long long)((head + i) % DIIS_SIZE) * dim; };
+    const double* last = hr + phys(count - 1);
+    int p = 0;
+    for (int j = count - 2; j >= 0; j--) {
+        double* d = basis + (long long)p * dim;
+        const double* rj = hr + phys(j);
+        double a = 0.0;
+        for (int i = tid; i < dim; i += nthr) {
+            double v = last[i] - rj[i];
+            d[i] = v;
+            a += v * v;
+        }
+        double norm0 = sqrt(cta_sum(a));
+        if (isnan(norm0) || norm0 <= 0.0) break;
+        for (int l = 0; l < p; l++) {
+            const double* bl = basis + (long long)l * dim;
+            double h = 0.0;
+            for (int i = tid; i < dim; i += nthr) h += bl[i] * d[i];
+            h = cta_sum(h);
+            if (tid == 0) s_R[l][p] = h;
+            for (int i = tid; i < dim; i += nthr) d[i] -= h * bl[i];
+        }
+        double b2 = 0.0;
+        for (int i = tid; i < dim; i += nthr) b2 += d[i] * d[i];
+        double nr = sqrt(cta_sum(b2));
+        if (nr < DIIS_DEPENDENCE * norm0) break;
+        if (tid == 0) {
+            s_R[p][p] = nr;
+            s_kept[p] = j;
+        }
+        for (int i = tid; i < dim; i += nthr) d[i] /= nr;
+        p++;
+    }
+    // R g = Q^T r_n by back substitution; c_j = g_j (kept j), c_n = 1 - sum g
+    for (int l = 0; l < p; l++) {
+        const double* bl = basis + (long long)l * dim;
+        double h = 0.0;
+        for (int i = tid; i < dim; i += nthr) h += bl[i] * last[i];
+        h = cta_sum(h);
+        if (tid == 0) s_g[l] = h;
+    }
+    if (tid == 0) {
+        for (int l = p - 1; l >= 0; l--) {
+            double v = s_g[l];
+            for (int k = l + 1; k < p; k++) v -= s_R[l][k] * s_g[k];
+            s_g[l] = v / s_R[l][l];
+        }
+        for (int i = 0; i < count; i++) s_c[i] = 0.0;
+        s_c[count - 1] = 1.0;
+        for (int l = 0; l < p; l++) {
+            s_c[s_kept[l]] += s_g[l];
+            s_c[count - 1] -= s_g[l];
         }
     }
     __syncthreads();
-    for (int a = tid; a < nat; a += nthr) {
-        double q = 0.0;
-        for (int s = B.a_sh0[a0 + a]; s < B.a_sh0[a0 + a] + B.a_nsh[a0 + a]; s++) q += S.qsh_in[s];
-        S.qat_in[a0 + a] = q;
+    for (int i = tid; i < dim; i += nthr) {
+        double x = 0.0;
+        for (int k = 0; k < count; k++) {
+            double c = s_c[k];
+            if (c != 0.0) x += c * (hq[phys(k) + i] + damp * hr[phys(k) + i]);
+        }
+        q_in[i] = x;
     }
+    unpack_input(B, S, m);
 }
 
 // ----------------------------------------------------------------------------- gradient pairs

@@ -56,6 +56,10 @@ typedef struct AxtbOptions {
                           C, P, mixer and sums stay FP64. For SCC accuracy >= ~1e-3; tighter
                           settings ask for energy changes below its rounding floor. */
     int32_t device;    /* CUDA device ordinal; 0 */
+    int32_t mixer;     /* SCC mixer (crates/axtb/src/scf/mixing.rs:81-94 MixerKind): 0 auto (default:
+                          modified Broyden; a molecule it leaves unconverged, with a failed mixer or a
+                          lost Fermi level starts again from its start moments with DIIS and another
+                          max_iter iterations), 1 Broyden alone, 2 DIIS alone */
 } AxtbOptions;
 
 /* Results of one single point (crates/base/src/method/results.rs:39-57). Array members are
@@ -70,11 +74,13 @@ typedef struct AxtbResult {
     double* qpat;           /* nat*6 atomic quadrupoles (xx, xy, yy, xz, yz, zz) */
     double terms[8];        /* repulsion, dispersion, electronic, isotropic_es, third_order,
                                anisotropic, entropy, band */
-    int32_t iterations;     /* SCF iterations */
+    int32_t iterations;     /* SCF iterations of the converged attempt (of all attempts on failure) */
     int32_t converged;      /* 1 when converged */
     int32_t status;         /* AxtbStatus of this molecule */
     double energy_change;   /* last |dE| (ScfNotConverged payload) */
     double residual;        /* last residual norm (ScfNotConverged payload) */
+    int32_t mixer_used;     /* mixer of the result (ScfResult::mixer_used): 0 Broyden, 1 DIIS,
+                               2 DIIS after Broyden did not converge ("diis-fallback") */
 } AxtbResult;
 
 /* One molecule of a batch: atomic numbers, positions (bohr, nat*3 row-major), charge and the

@@ -27,6 +27,11 @@ enum AxtbDebugQuantity {
     AXTB_DBG_LINV = 11,       /* nao*nao inverse Cholesky factor of the overlap */
     AXTB_DBG_EIGEN_CYCLES = 12, /* 1 value: SM clock cycles of the molecule's last eigen phase
                                    (runs with profiling on; 0 otherwise) */
+    AXTB_DBG_STATUS_BITS = 13,  /* 1 value: the molecule's raw status bits of its last attempt
+                                   (1 overlap/EEQ not positive definite, 2 non-finite energy,
+                                   4 Fermi level lost, 8 mixer failed, 16 non-finite
+                                   inverse-iteration vector, 32 Broyden history full, 64 a
+                                   bounded device wait gave up, 128 non-finite Fock matrix) */
 };
 
 /* Per-kernel timing: with profiling on, every kernel launch of a run is bracketed by CUDA

@@ -22,6 +22,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1609,18 +1611,31 @@ double entropy_tblite(const vector<double>& occ, double kt) {
 // ============================================================================ Broyden
 // modified Broyden mixing of crates/axtb/src/scf/mixing.rs:185-338 (memory = max_iter) with
 // Gauss elimination crates/base/src/linalg/lu.rs:81-112
-struct Broyden {
+// sequential dot product (crates/base/src/math.rs:69-71)
+double dot_seq(const vector<double>& x, const vector<double>& y) {
+    double s = -0.0;
+    for (size_t i = 0; i < x.size(); i++) s += x[i] * y[i];
+    return s;
+}
+
+// a mixer of the packed SCC variables (crates/axtb/src/scf/mixing.rs:27-39 VectorMixer): the
+// SCF writes the input q_in it built the Fock matrix from and the residual dq = out - q_in, and
+// next() replaces q_in by the next input (false: the mixer failed)
+struct VMix {
+    vector<double> q_in, dq;
+    explicit VMix(int n) : q_in(n), dq(n) {}
+    virtual ~VMix() = default;
+    virtual bool next() = 0;
+};
+
+struct Broyden : VMix {
     int n, memory, iter = 0;
     double damp;
     vector<vector<double>> df, u, a;
-    vector<double> omega, q_in, dq, qlast, dqlast;
-    Broyden(int n_, int mem, double d) : n(n_), memory(std::max(mem, 1)), damp(d), q_in(n_), dq(n_), qlast(n_), dqlast(n_) {}
-    static double dot(const vector<double>& x, const vector<double>& y) {
-        double s = -0.0;
-        for (size_t i = 0; i < x.size(); i++) s += x[i] * y[i];
-        return s;
-    }
-    bool next() {
+    vector<double> omega, qlast, dqlast;
+    Broyden(int n_, int mem, double d) : VMix(n_), n(n_), memory(std::max(mem, 1)), damp(d), qlast(n_), dqlast(n_) {}
+    static double dot(const vector<double>& x, const vector<double>& y) { return dot_seq(x, y); }
+    bool next() override {
         iter++;
         if (iter == 1) {
             dqlast = dq;
@@ -1693,6 +1708,108 @@ struct Broyden {
     }
 };
 
+// ============================================================================ DIIS
+// Pulay (DIIS / Anderson) mixing with restarts (crates/axtb/src/scf/mixing.rs:342-525): the
+// constants of :342-357, next() of :414-458 and the coefficients of :466-525.
+const int DIIS_SIZE = 30;
+const double DIIS_DEPENDENCE = 1e-2;
+const int DIIS_STALL = 12;
+const double DIIS_RESTART_GROWTH = 1e3, DIIS_RESTART_FLOOR = 0.1;
+
+// c minimising |sum_i c_i r_i| with sum_i c_i = 1, from min_g |r_n - sum_j g_j (r_n - r_j)|:
+// the differences to the newest residual are orthonormalised newest first by modified
+// Gram-Schmidt until one keeps less than DIIS_DEPENDENCE of its norm; R g = Q^T r_n is solved by
+// back substitution, c_j = g_j for the kept j and c_n = 1 - sum g
+vector<double> diis_coefficients(const std::deque<vector<double>>& r) {
+    int m = (int)r.size();
+    const vector<double>& last = r[m - 1];
+    size_t n = last.size();
+    vector<vector<double>> basis, rcol;
+    vector<int> kept;
+    for (int j = m - 2; j >= 0; j--) {
+        vector<double> d(n);
+        for (size_t k = 0; k < n; k++) d[k] = last[k] - r[j][k];
+        double norm0 = std::sqrt(dot_seq(d, d));
+        if (std::isnan(norm0) || norm0 <= 0.0) break;
+        vector<double> col(basis.size() + 1, 0.0);
+        for (size_t l = 0; l < basis.size(); l++) {
+            double h = dot_seq(basis[l], d);
+            col[l] = h;
+            for (size_t k = 0; k < n; k++) d[k] -= h * basis[l][k];
+        }
+        double nr = std::sqrt(dot_seq(d, d));
+        if (nr < DIIS_DEPENDENCE * norm0) break;
+        col[basis.size()] = nr;
+        for (double& x : d) x /= nr;
+        basis.push_back(std::move(d));
+        rcol.push_back(std::move(col));
+        kept.push_back(j);
+    }
+    int p = (int)basis.size();
+    vector<double> g(p, 0.0);
+    for (int l = p - 1; l >= 0; l--) {
+        double v = dot_seq(basis[l], last);
+        for (int k = l + 1; k < p; k++) v -= rcol[k][l] * g[k];
+        g[l] = v / rcol[l][l];
+    }
+    vector<double> c(m, 0.0);
+    c[m - 1] = 1.0;
+    for (int l = 0; l < p; l++) {
+        c[kept[l]] += g[l];
+        c[m - 1] -= g[l];
+    }
+    return c;
+}
+
+struct Diis : VMix {
+    double damp;
+    std::deque<vector<double>> hq, hr;
+    bool have_best = false;
+    double best_norm = 0.0;
+    vector<double> best_q, best_r;
+    int since_best = 0;
+    Diis(int n, double d) : VMix(n), damp(d) {}
+    bool next() override {
+        double norm = std::sqrt(dot_seq(dq, dq));
+        if (!std::isfinite(norm)) return false;
+        if (have_best) {
+            bool diverging = norm > DIIS_RESTART_GROWTH * best_norm && norm > DIIS_RESTART_FLOOR;
+            if (diverging || since_best >= DIIS_STALL) {
+                // restart from the best iterate with half the damping
+                since_best = 0;
+                hq.clear();
+                hr.clear();
+                damp *= 0.5;
+                for (size_t k = 0; k < best_q.size(); k++) q_in[k] = best_q[k] + damp * best_r[k];
+                return true;
+            }
+        }
+        if (!have_best || norm < best_norm) {
+            have_best = true;
+            best_norm = norm;
+            best_q = q_in;
+            best_r = dq;
+            since_best = 0;
+        } else {
+            since_best++;
+        }
+        if ((int)hq.size() == DIIS_SIZE) {
+            hq.pop_front();
+            hr.pop_front();
+        }
+        hq.push_back(q_in);
+        hr.push_back(dq);
+        vector<double> c = diis_coefficients(hr);
+        for (size_t k = 0; k < q_in.size(); k++) {
+            double x = 0.0;
+            for (size_t i = 0; i < c.size(); i++)
+                if (c[i] != 0.0) x += c[i] * (hq[i][k] + damp * hr[i][k]);
+            q_in[k] = x;
+        }
+        return true;
+    }
+};
+
 // ============================================================================ single point
 const double SQRT2 = 1.4142135623730951;
 const bool QOFF[6] = {false, true, false, true, true, false};
@@ -1750,6 +1867,7 @@ int run(OracleRun* R) {
     }
     double acc = R->accuracy;
     if (!(acc > 0.0)) throw Fail(1, "accuracy must be positive");
+    if (R->mixer < 0 || R->mixer > 2) throw Fail(1, "unknown SCF mixer (auto, broyden or diis)");
     Model md = build_model(m, acc);
     const Basis& b = md.b;
     int nat = m.nat, nsh = b.nsh, nao = b.nao;
@@ -1803,7 +1921,6 @@ int run(OracleRun* R) {
     qat_from_qsh(b, nat, st.qsh, st.qat);
 
     int ndim = nsh + 9 * nat;
-    Broyden mix(ndim, R->max_iter, 0.4);
     const double econv = 1e-6 * acc, pconv = 2e-5 * acc;
     Pot pot;
     vector<double> F((size_t)nao * nao), C, emo, occa(nao), occb(nao), focc(nao), P((size_t)nao * nao);
@@ -1812,130 +1929,155 @@ int run(OracleRun* R) {
     double terms[8] = {0};
     Moments out;
     bool converged = false;
-    int iters = 0;
-    Moments state = st;
+    int iters = 0, iters_all = 0;
     vector<double> packed;
-    for (int iter = 1; iter <= R->max_iter; iter++) {
-        if (iter > 1) {
-            if (!mix.next()) throw Fail(4, "Broyden mixing failed");
-            unpack(mix.q_in, b, nat, state);
-        }
-        iters = iter;
-        // potentials (xtb.rs:316-340)
-        pot.vsh.assign(nsh, 0.0);
-        pot.vat.assign(nat, 0.0);
-        pot.vdp.assign(3 * nat, 0.0);
-        pot.vqp.assign(6 * nat, 0.0);
-        for (int a = 0; a < nsh; a++) {
-            double s = 0.0;
-            for (int c = 0; c < nsh; c++) s += gam[(size_t)a * nsh + c] * state.qsh[c];
-            pot.vsh[a] += s;
-        }
-        for (int a = 0; a < nsh; a++) pot.vsh[a] += state.qsh[a] * state.qsh[a] * md.gam3[a];
-        aes_potential(md, ac, state.qat, state.dp, state.qp, pot.vat, pot.vdp, pot.vqp);
-        d4_energy(d4, state.qat, &pot.vat);
-        // Fock (crates/axtb/src/scf/fock.rs:22-104)
-        vector<double> B((size_t)nao * nao);
-        for (int nu = 0; nu < nao; nu++) {
-            int at = b.ao2at[nu];
-            double v = pot.vsh[b.ao2sh[nu]] + pot.vat[at];
-            for (int mu = 0; mu < nao; mu++) {
-                size_t k = (size_t)mu + (size_t)nu * nao;
-                double x = I.S[k] * v;
-                for (int c = 0; c < 3; c++) x += I.D[c][k] * pot.vdp[3 * at + c];
-                for (int c = 0; c < 6; c++) x += I.Q[c][k] * pot.vqp[6 * at + c];
-                B[k] = x;
+    // the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199, run by
+    // crates/axtb/src/xtb.rs:590-645): auto = Broyden, then DIIS from the start guess with its own
+    // max_iter; a failed mixer or a lost Fermi level gives way to the next attempt and ends the
+    // last one with its error (non-finite values end the single point at once)
+    const int plan_auto[2] = {1, 2}, plan_broyden[1] = {1}, plan_diis[1] = {2};
+    const int* plan = R->mixer == 1 ? plan_broyden : R->mixer == 2 ? plan_diis : plan_auto;
+    int nplan = R->mixer == 0 ? 2 : 1;
+    for (int ia = 0; ia < nplan && !converged; ia++) {
+        bool last_attempt = ia + 1 == nplan;
+        std::unique_ptr<VMix> mixer;
+        if (plan[ia] == 1) mixer.reset(new Broyden(ndim, R->max_iter, 0.4));
+        else mixer.reset(new Diis(ndim, 0.4));
+        VMix& mix = *mixer;
+        Moments state = st;
+        elast = 0.0;
+        iters = 0;
+        for (int iter = 1; iter <= R->max_iter; iter++) {
+            if (iter > 1) {
+                if (!mix.next()) {
+                    if (last_attempt) throw Fail(4, plan[ia] == 1 ? "Broyden mixing failed" : "DIIS mixing failed");
+                    break;
+                }
+                unpack(mix.q_in, b, nat, state);
             }
-        }
-        for (int nu = 0; nu < nao; nu++)
-            for (int mu = 0; mu < nao; mu++) {
-                size_t k = (size_t)mu + (size_t)nu * nao;
-                F[k] = I.H0[k] - 0.5 * (B[k] + B[(size_t)nu + (size_t)mu * nao]);
-                if (!std::isfinite(F[k])) throw Fail(4, "non-finite Fock matrix");
+            iters = iter;
+            // potentials (xtb.rs:316-340)
+            pot.vsh.assign(nsh, 0.0);
+            pot.vat.assign(nat, 0.0);
+            pot.vdp.assign(3 * nat, 0.0);
+            pot.vqp.assign(6 * nat, 0.0);
+            for (int a = 0; a < nsh; a++) {
+                double s = 0.0;
+                for (int c = 0; c < nsh; c++) s += gam[(size_t)a * nsh + c] * state.qsh[c];
+                pot.vsh[a] += s;
             }
-        pack(state, nsh, nat, mix.q_in);
-        // diagonalize + fill (xtb.rs:997-1031)
-        eig.solve(F, emo, C);
-        double efa = 0, efb = 0;
-        fill_tblite(nalpha, kt, emo, occa, efa);
-        fill_tblite(nbeta, kt, emo, occb, efb);
-        kocc = 0;
-        for (int i = nao - 1; i >= 0; i--)
-            if (occa[i] + occb[i] > 1e-16) {
-                kocc = i + 1;
+            for (int a = 0; a < nsh; a++) pot.vsh[a] += state.qsh[a] * state.qsh[a] * md.gam3[a];
+            aes_potential(md, ac, state.qat, state.dp, state.qp, pot.vat, pot.vdp, pot.vqp);
+            d4_energy(d4, state.qat, &pot.vat);
+            // Fock (crates/axtb/src/scf/fock.rs:22-104)
+            vector<double> B((size_t)nao * nao);
+            for (int nu = 0; nu < nao; nu++) {
+                int at = b.ao2at[nu];
+                double v = pot.vsh[b.ao2sh[nu]] + pot.vat[at];
+                for (int mu = 0; mu < nao; mu++) {
+                    size_t k = (size_t)mu + (size_t)nu * nao;
+                    double x = I.S[k] * v;
+                    for (int c = 0; c < 3; c++) x += I.D[c][k] * pot.vdp[3 * at + c];
+                    for (int c = 0; c < 6; c++) x += I.Q[c][k] * pot.vqp[6 * at + c];
+                    B[k] = x;
+                }
+            }
+            for (int nu = 0; nu < nao; nu++)
+                for (int mu = 0; mu < nao; mu++) {
+                    size_t k = (size_t)mu + (size_t)nu * nao;
+                    F[k] = I.H0[k] - 0.5 * (B[k] + B[(size_t)nu + (size_t)mu * nao]);
+                    if (!std::isfinite(F[k])) throw Fail(4, "non-finite Fock matrix");
+                }
+            pack(state, nsh, nat, mix.q_in);
+            // diagonalize + fill (xtb.rs:997-1031)
+            eig.solve(F, emo, C);
+            double efa = 0, efb = 0;
+            fill_tblite(nalpha, kt, emo, occa, efa);
+            fill_tblite(nbeta, kt, emo, occb, efb);
+            kocc = 0;
+            for (int i = nao - 1; i >= 0; i--)
+                if (occa[i] + occb[i] > 1e-16) {
+                    kocc = i + 1;
+                    break;
+                }
+            double pa = 0, pb = 0;
+            for (int i = 0; i < nao; i++) {
+                pa += occa[i];
+                pb += occb[i];
+            }
+            if (std::fabs(pa - nalpha) > 1e-6 || std::fabs(pb - nbeta) > 1e-6) {
+                if (last_attempt) throw Fail(4, "Fermi level not found");
                 break;
             }
-        double pa = 0, pb = 0;
-        for (int i = 0; i < nao; i++) {
-            pa += occa[i];
-            pb += occb[i];
-        }
-        if (std::fabs(pa - nalpha) > 1e-6 || std::fabs(pb - nbeta) > 1e-6) throw Fail(4, "Fermi level not found");
-        ts = entropy_tblite(occa, kt) + entropy_tblite(occb, kt);
-        for (int i = 0; i < nao; i++) focc[i] = occa[i] + occb[i];
-        // density (occupied columns)
-        std::fill(P.begin(), P.end(), 0.0);
-        for (int k = 0; k < kocc; k++) {
-            double f = focc[k];
-            const double* c = &C[(size_t)k * nao];
+            ts = entropy_tblite(occa, kt) + entropy_tblite(occb, kt);
+            for (int i = 0; i < nao; i++) focc[i] = occa[i] + occb[i];
+            // density (occupied columns)
+            std::fill(P.begin(), P.end(), 0.0);
+            for (int k = 0; k < kocc; k++) {
+                double f = focc[k];
+                const double* c = &C[(size_t)k * nao];
+                for (int nu = 0; nu < nao; nu++) {
+                    double fc = f * c[nu];
+                    for (int mu = 0; mu < nao; mu++) P[(size_t)mu + (size_t)nu * nao] += c[mu] * fc;
+                }
+            }
+            // Mulliken (crates/axtb/src/scf/mulliken.rs:19-59)
+            out.qsh.assign(md.refocc.begin(), md.refocc.end());
+            out.dp.assign(3 * nat, 0.0);
+            out.qp.assign(6 * nat, 0.0);
             for (int nu = 0; nu < nao; nu++) {
-                double fc = f * c[nu];
-                for (int mu = 0; mu < nao; mu++) P[(size_t)mu + (size_t)nu * nao] += c[mu] * fc;
+                int at = b.ao2at[nu];
+                double r0 = 0.0, r[9] = {0};
+                for (int mu = 0; mu < nao; mu++) {
+                    size_t k = (size_t)mu + (size_t)nu * nao;
+                    r0 += P[k] * I.S[k];
+                    for (int c = 0; c < 3; c++) r[c] += P[k] * I.D[c][k];
+                    for (int c = 0; c < 6; c++) r[3 + c] += P[k] * I.Q[c][k];
+                }
+                out.qsh[b.ao2sh[nu]] -= r0;
+                for (int c = 0; c < 3; c++) out.dp[3 * at + c] -= r[c];
+                for (int c = 0; c < 6; c++) out.qp[6 * at + c] -= r[3 + c];
+            }
+            qat_from_qsh(b, nat, out.qsh, out.qat);
+            pack(out, nsh, nat, packed);
+            for (int i = 0; i < ndim; i++) mix.dq[i] = packed[i] - mix.q_in[i];
+            // energy (xtb.rs:1058-1146)
+            double e2 = 0.0;
+            for (int a = 0; a < nsh; a++) {
+                double v = 0.0;
+                for (int c = 0; c < nsh; c++) v += gam[(size_t)a * nsh + c] * out.qsh[c];
+                e2 += 0.5 * out.qsh[a] * v;
+            }
+            double e3 = 0.0;
+            for (int a = 0; a < nsh; a++) e3 += out.qsh[a] * out.qsh[a] * out.qsh[a] * md.gam3[a] / 3.0;
+            double eaes = aes_energy(md, ac, out.qat, out.dp, out.qp);
+            double edisp = d4_energy(d4, out.qat, nullptr);
+            double band = 0.0;
+            for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
+            double energy = e2 + e3 + eaes + edisp + ts + band;
+            if (!std::isfinite(energy)) throw Fail(4, "non-finite energy");
+            double res = 0.0;
+            for (double x : mix.dq) res += x * x;
+            res = std::sqrt(res / ndim);
+            double de = energy - elast;
+            elast = energy;
+            terms[2] = energy;
+            terms[3] = e2;
+            terms[4] = e3;
+            terms[5] = eaes;
+            terms[1] = edisp;
+            terms[6] = ts;
+            terms[7] = band;
+            if (std::fabs(de) < econv && res < pconv) {
+                converged = true;
+                break;
             }
         }
-        // Mulliken (crates/axtb/src/scf/mulliken.rs:19-59)
-        out.qsh.assign(md.refocc.begin(), md.refocc.end());
-        out.dp.assign(3 * nat, 0.0);
-        out.qp.assign(6 * nat, 0.0);
-        for (int nu = 0; nu < nao; nu++) {
-            int at = b.ao2at[nu];
-            double r0 = 0.0, r[9] = {0};
-            for (int mu = 0; mu < nao; mu++) {
-                size_t k = (size_t)mu + (size_t)nu * nao;
-                r0 += P[k] * I.S[k];
-                for (int c = 0; c < 3; c++) r[c] += P[k] * I.D[c][k];
-                for (int c = 0; c < 6; c++) r[3 + c] += P[k] * I.Q[c][k];
-            }
-            out.qsh[b.ao2sh[nu]] -= r0;
-            for (int c = 0; c < 3; c++) out.dp[3 * at + c] -= r[c];
-            for (int c = 0; c < 6; c++) out.qp[6 * at + c] -= r[3 + c];
-        }
-        qat_from_qsh(b, nat, out.qsh, out.qat);
-        pack(out, nsh, nat, packed);
-        for (int i = 0; i < ndim; i++) mix.dq[i] = packed[i] - mix.q_in[i];
-        // energy (xtb.rs:1058-1146)
-        double e2 = 0.0;
-        for (int a = 0; a < nsh; a++) {
-            double v = 0.0;
-            for (int c = 0; c < nsh; c++) v += gam[(size_t)a * nsh + c] * out.qsh[c];
-            e2 += 0.5 * out.qsh[a] * v;
-        }
-        double e3 = 0.0;
-        for (int a = 0; a < nsh; a++) e3 += out.qsh[a] * out.qsh[a] * out.qsh[a] * md.gam3[a] / 3.0;
-        double eaes = aes_energy(md, ac, out.qat, out.dp, out.qp);
-        double edisp = d4_energy(d4, out.qat, nullptr);
-        double band = 0.0;
-        for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
-        double energy = e2 + e3 + eaes + edisp + ts + band;
-        if (!std::isfinite(energy)) throw Fail(4, "non-finite energy");
-        double res = 0.0;
-        for (double x : mix.dq) res += x * x;
-        res = std::sqrt(res / ndim);
-        double de = energy - elast;
-        elast = energy;
-        terms[2] = energy;
-        terms[3] = e2;
-        terms[4] = e3;
-        terms[5] = eaes;
-        terms[1] = edisp;
-        terms[6] = ts;
-        terms[7] = band;
-        if (std::fabs(de) < econv && res < pconv) {
-            converged = true;
-            break;
-        }
+        iters_all += iters;
+        R->mixer_used = plan[ia] == 1 ? 0 : (R->mixer == 0 ? 2 : 1);
     }
-    R->iterations = iters;
+    // iterations of the converged attempt; of all attempts when none converged (xtb.rs:624-645)
+    R->iterations = converged ? iters : iters_all;
     R->converged = converged;
     terms[0] = e_rep;
     terms[1] += e_atm;
@@ -2065,6 +2207,7 @@ extern "C" int oracle_singlepoint(OracleRun* R) {
     R->error[0] = 0;
     R->iterations = 0;
     R->converged = 0;
+    R->mixer_used = 0;
     try {
         return run(R);
     } catch (const Fail& f) {
@@ -2073,6 +2216,33 @@ extern "C" int oracle_singlepoint(OracleRun* R) {
     } catch (const std::exception& e) {
         std::snprintf(R->error, sizeof R->error, "%s", e.what());
         return 4;
+    }
+}
+
+// the DIIS mixer alone, for its own tests (crates/axtb/src/scf/mixing.rs:583-652): coefficients
+// of m residuals of length n (row i = r_i, oldest first)
+extern "C" void oracle_diis_coefficients(int m, int n, const double* r, double* c) {
+    std::deque<vector<double>> h;
+    for (int i = 0; i < m; i++) h.emplace_back(r + (size_t)i * n, r + (size_t)(i + 1) * n);
+    vector<double> v = diis_coefficients(h);
+    std::copy(v.begin(), v.end(), c);
+}
+
+// DIIS on the linear fixed point q = diag(eig) q + b from q = 0: steps until the RMS residual is
+// below tol (or -1 after max_steps, or -2 when the mixer failed); the last input in q
+extern "C" int oracle_diis_linear(int n, const double* eig, const double* b, double damp, double tol, int max_steps,
+                                  double* q) {
+    Diis mix(n, damp);
+    for (int step = 0;; step++) {
+        double rr = 0.0;
+        for (int k = 0; k < n; k++) {
+            mix.dq[k] = eig[k] * mix.q_in[k] + b[k] - mix.q_in[k];
+            rr += mix.dq[k] * mix.dq[k];
+        }
+        std::copy(mix.q_in.begin(), mix.q_in.end(), q);
+        if (std::sqrt(rr / n) < tol) return step;
+        if (step == max_steps) return -1;
+        if (!mix.next()) return -2;
     }
 }
 

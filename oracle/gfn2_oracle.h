@@ -27,6 +27,7 @@ typedef struct {
     int want_gradient;
     int eig_backend;         /* 0: builtin Householder/QL, 1: dlopen'ed LAPACK when found */
     int lapack_threads;      /* threads of the LAPACK backend (0 = library default) */
+    int mixer;               /* 0: auto (Broyden, then DIIS from the start guess), 1: Broyden, 2: DIIS */
     /* outputs (caller-allocated; any may be NULL) */
     double* energy;
     double* gradient;        /* nat*3 */
@@ -41,8 +42,9 @@ typedef struct {
     double* focc;            /* nao occupations */
     double* density;         /* nao*nao, column-major */
     double* wdensity;        /* nao*nao */
-    int iterations;
+    int iterations;          /* of the converged attempt; of all attempts when none converged */
     int converged;
+    int mixer_used;          /* mixer of the last attempt: 0 Broyden, 1 DIIS, 2 DIIS after Broyden (auto) */
     int nsh, nao;
     char error[256];
 } OracleRun;
@@ -59,6 +61,14 @@ int oracle_singlepoint(OracleRun* run);
  * any pointer may be NULL) at SCF accuracy acc. */
 int oracle_integrals(int nat, const int* numbers, const double* positions, double acc,
                      double* cn, double* S, double* H0, double* D, double* Q);
+
+/* The DIIS mixer alone: Pulay coefficients of m residuals of length n (row-major, oldest
+ * first) into c (m); and DIIS on the linear fixed point q = diag(eig) q + b from q = 0, returning
+ * the steps until the RMS residual is below tol (-1: not within max_steps, -2: mixer failed)
+ * with the last input in q (n). */
+void oracle_diis_coefficients(int m, int n, const double* r, double* c);
+int oracle_diis_linear(int n, const double* eig, const double* b, double damp, double tol, int max_steps,
+                       double* q);
 
 #ifdef __cplusplus
 }

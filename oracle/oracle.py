@@ -23,17 +23,21 @@ class _Run(C.Structure):
         ("nat", C.c_int), ("numbers", C.POINTER(C.c_int)), ("positions", C.POINTER(C.c_double)),
         ("charge", C.c_double), ("uhf", C.c_int), ("accuracy", C.c_double), ("etemp", C.c_double),
         ("max_iter", C.c_int), ("want_gradient", C.c_int), ("eig_backend", C.c_int),
-        ("lapack_threads", C.c_int),
+        ("lapack_threads", C.c_int), ("mixer", C.c_int),
         ("energy", C.POINTER(C.c_double)), ("gradient", C.POINTER(C.c_double)),
         ("qat", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)),
         ("dpat", C.POINTER(C.c_double)), ("qpat", C.POINTER(C.c_double)),
         ("dipole", C.POINTER(C.c_double)), ("terms", C.POINTER(C.c_double)),
         ("emo", C.POINTER(C.c_double)), ("focc", C.POINTER(C.c_double)),
         ("density", C.POINTER(C.c_double)), ("wdensity", C.POINTER(C.c_double)),
-        ("iterations", C.c_int), ("converged", C.c_int), ("nsh", C.c_int), ("nao", C.c_int),
+        ("iterations", C.c_int), ("converged", C.c_int), ("mixer_used", C.c_int), ("nsh", C.c_int),
+        ("nao", C.c_int),
         ("error", C.c_char * 256),
     ]
 
+
+MIXERS = {"auto": 0, "broyden": 1, "diis": 2}
+MIXER_USED = ("broyden", "diis", "diis-fallback")
 
 TERM_NAMES = ("repulsion", "dispersion", "electronic", "isotropic_es", "third_order", "anisotropic",
               "entropy", "band")
@@ -59,7 +63,28 @@ def lib():
         _lib.oracle_sizes.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         _lib.oracle_integrals.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_double] + \
             [C.POINTER(C.c_double)] * 5
+        _lib.oracle_diis_coefficients.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _lib.oracle_diis_coefficients.restype = None
+        _lib.oracle_diis_linear.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                            C.c_double, C.c_int, C.POINTER(C.c_double)]
     return _lib
+
+
+def diis_coefficients(residuals):
+    """Pulay coefficients of the residuals (rows, oldest first) by the oracle's DIIS."""
+    r = np.ascontiguousarray(residuals, dtype=np.float64)
+    c = np.zeros(r.shape[0])
+    lib().oracle_diis_coefficients(r.shape[0], r.shape[1], _p(r), _p(c))
+    return c
+
+
+def diis_linear(eig, b, damp=0.4, tol=1e-12, max_steps=100):
+    """DIIS on q = diag(eig) q + b from q = 0: (steps or -1/-2, last input)."""
+    e = np.ascontiguousarray(eig, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    q = np.zeros(len(e))
+    steps = lib().oracle_diis_linear(len(e), _p(e), _p(bb), float(damp), float(tol), int(max_steps), _p(q))
+    return steps, q
 
 
 def _p(a):
@@ -75,9 +100,11 @@ def sizes(numbers):
 
 
 def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=300.0, max_iter=250,
-                gradient=True, matrices=False, lapack=False, lapack_threads=1):
+                gradient=True, matrices=False, lapack=False, lapack_threads=1, mixer="auto", failed=False):
     """Run the oracle; returns a dict (energy, gradient, qat, qsh, dpat, qpat, dipole, terms, emo,
-    focc, iterations, converged[, density, wdensity]). Raises RuntimeError on a failed SCF."""
+    focc, iterations, converged, mixer_used[, density, wdensity]). ``mixer``: "auto" (Broyden,
+    then DIIS from the start guess), "broyden" or "diis". Raises RuntimeError on a failed SCF
+    unless ``failed`` (then the dict of the failed run carries ``status`` and ``error``)."""
     z = np.ascontiguousarray(numbers, dtype=np.int32)
     x = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
     nat = len(z)
@@ -102,14 +129,18 @@ def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=30
     r.want_gradient = int(bool(gradient))
     r.eig_backend = 1 if lapack else 0
     r.lapack_threads = int(lapack_threads)
+    r.mixer = MIXERS[mixer]
     for k in ("energy", "gradient", "qat", "qsh", "dpat", "qpat", "dipole", "terms", "emo", "focc"):
         setattr(r, k, _p(out[k]))
     if matrices:
         r.density = _p(out["density"])
         r.wdensity = _p(out["wdensity"])
     rc = lib().oracle_singlepoint(C.byref(r))
-    if rc != 0:
+    if rc != 0 and not failed:
         raise RuntimeError(f"oracle status {rc}: {r.error.decode()}")
+    out["status"] = rc
+    out["error"] = r.error.decode()
+    out["mixer_used"] = MIXER_USED[r.mixer_used]
     out["energy"] = float(out["energy"][0])
     out["terms"] = dict(zip(TERM_NAMES, out["terms"].tolist()))
     out["iterations"] = r.iterations
