@@ -81,24 +81,36 @@ class _ResultBuffers:
                            residual=r.residual, mixer_used=MIXER_USED[r.mixer_used])
 
 
-# SCC mixers by name (crates/axtb/src/scf/mixing.rs:202-214: case-insensitive, "pulay" = DIIS)
+# SCC mixers by name (crates/axtb/src/scf/mixing.rs:202-214: case-insensitive, "pulay" = DIIS;
+# None: the conventions' own)
 MIXERS = {"auto": 0, "broyden": 1, "diis": 2, "pulay": 2}
+# conventions by name (crates/axtb/src/conventions.rs; the xtb 6.7.1 row is not built)
+CONVENTIONS = {"axtb": 0, "xtb": 1, "tblite": 2}
 MIXER_USED = ("broyden", "diis", "diis-fallback")
 
 
-def _mixer(name: str) -> int:
+def _mixer(name) -> int:
+    if name is None:
+        return -1
     try:
         return MIXERS[name.lower()]
     except KeyError:
         raise AxtbError(1, f"unknown SCF mixer {name!r} (auto, broyden or diis)") from None
 
 
+def _conventions(name: str) -> int:
+    try:
+        return CONVENTIONS[name.lower()]
+    except KeyError:
+        raise AxtbError(1, f"unknown conventions {name!r} (axtb, xtb or tblite)") from None
+
+
 def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0,
-             mixer="auto"):
+             mixer=None, conventions="axtb"):
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
                                 damping=float(damping), guess=0 if guess == "eeq" else 1,
                                 precision={"fp64": 0, "split": 1}[precision], device=int(device),
-                                mixer=_mixer(mixer))
+                                mixer=_mixer(mixer), conventions=_conventions(conventions))
 
 
 class Calculator:

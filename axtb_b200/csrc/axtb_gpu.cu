@@ -111,6 +111,67 @@ HShell sto_shell(int z, int ish) {
 double rcov_codata(int z) { return 4.0 / 3.0 * (gfn2tab::COVALENT_RAD_2009_AA[z - 1] * AATOAU); }
 double rcov_mctc(int z) { return 4.0 / 3.0 * (MCTC_AATOAU * gfn2tab::COVALENT_RAD_2009_AA[z - 1]); }
 
+// ------------------------------------------------------------------ conventions
+// The settings that differ between axtb's default conventions, the xtb 6.8.0 program's and
+// tblite 0.8.0's (crates/axtb/src/conventions.rs:150-353 ConventionParams): Boltzmann constant
+// and aufbau limit, EEQ start and its CN, element tables, real-space cutoffs, integral
+// screening, default mixer and the potentials of the gradient. Not carried over: the per-triple
+// ATM order and the full eigensolver of the program conventions (the same numbers up to
+// round-off as the pair sums and occupied-only solve used for all three), and the xtb 6.7.1 row.
+const double KB_XTB_TBLITE = 3.166808578545117e-06;  // crates/base/src/units.rs:81
+struct Conv {
+    int id = 0;  // 0 axtb, 1 xtb (6.8.0), 2 tblite (0.8.0)
+    double kb = KB_HARTREE, aufbau_max_etemp = 0.0;
+    bool eeq_guess = true;
+    double eeq_cn_cut = 25.0, eeq_cap = 8.0;
+    double cn_cut = 40.0, rep_cut = 40.0, d4_cn_cut = 40.0, d2_cut = 72.0, d2_w = 1.0, d3_cut = 40.0, d3_w = 1.0;
+    bool output_aes = false;
+    int default_mixer = 0;  // 0 auto, 1 Broyden
+    explicit Conv(int c) : id(c) {
+        if (c == 0) return;
+        kb = KB_XTB_TBLITE;
+        cn_cut = rep_cut = 25.0;
+        d4_cn_cut = 30.0;  // RealspaceCutoff::TBLITE_GFN2 (crates/d4/src/disp.rs:44-47)
+        d2_cut = 50.0;
+        d3_cut = 25.0;
+        d2_w = d3_w = 0.05;
+        default_mixer = 1;
+        if (c == 1) {
+            aufbau_max_etemp = 0.1;
+            eeq_cn_cut = 40.0;  // the xtb program's guess CN: its D4 radii, 40 bohr, no cap
+            eeq_cap = 0.0;
+            output_aes = true;
+        } else {
+            eeq_guess = false;
+        }
+    }
+    double en(int z) const { return id == 1 ? gfn2tab::XTB_PAULING_EN[z - 1] : gfn2tab::PAULING_EN[z - 1]; }
+    double atomic_rad(int z) const {
+        return id == 1 ? gfn2tab::XTB_ATOMIC_RAD[z - 1]
+                       : id == 2 ? MCTC_AATOAU * ATOMIC_RAD_AA[z - 1] : ATOMIC_RAD_AA[z - 1] * AATOAU;
+    }
+    double cn_rcov(int z) const {
+        return id == 1 ? gfn2tab::XTB_COVALENT_RAD_D3[z - 1] : id == 2 ? rcov_mctc(z) : rcov_codata(z);
+    }
+    double d4_rcov(int z) const { return id == 1 ? gfn2tab::XTB_D4_RCOV[z - 1] : id == 2 ? rcov_mctc(z) : rcov_codata(z); }
+    double d4_en(int z) const { return id == 1 ? gfn2tab::XTB_D4_EN[z - 1] : gfn2tab::PAULING_EN[z - 1]; }
+    double eeq_rcov(int z) const { return id == 1 ? gfn2tab::XTB_D4_RCOV[z - 1] : rcov_mctc(z); }
+    // primitive screening (crates/axtb/src/gfn2.rs:58-62, crates/axtb/src/basis.rs:135-143)
+    static double tblite_cut(double acc) {
+        acc = std::min(std::max(acc, 1.0e-4), 1.0e3);
+        return std::min(std::max(25.0 - 10.0 * std::log10(acc), 5.0), 25.0);
+    }
+    double intcut(double acc) const {
+        return id == 0 ? std::max(25.0 - 10.0 * std::log10(acc), 20.0) : id == 1 ? tblite_cut(acc) : tblite_cut(1.0);
+    }
+    // tblite's atom-pair cutoff of the integrals, squared (crates/axtb/src/basis.rs:247-249)
+    double pair_cut2(double acc, double min_alpha) const {
+        if (id != 2) return INFINITY;
+        double pc = std::min(std::sqrt(2.0 * tblite_cut(acc) / min_alpha), 40.0);
+        return pc * pc;
+    }
+};
+
 struct HostMol {
     int nat = 0;
     vector<int> Z;
@@ -172,7 +233,8 @@ void check_molecule(HostMol& m) {
 struct Opt {
     double acc = 1.0, etemp = 300.0, damping = 0.4;
     int max_iter = 250, guess = 0, precision = 0, device = 0;
-    int mixer = 0;  // 0 auto (Broyden, then DIIS from the start), 1 Broyden, 2 DIIS
+    int mixer = -1;  // -1 the conventions' mixer, 0 auto (Broyden, then DIIS from the start), 1 Broyden, 2 DIIS
+    int conventions = 0;  // 0 axtb, 1 xtb (6.8.0), 2 tblite (0.8.0)
 };
 
 void check_options(const Opt& o) {
@@ -181,7 +243,8 @@ void check_options(const Opt& o) {
     if (!(o.damping > 0.0 && o.damping <= 1.0)) throw Fail(AXTB_ERR_INPUT, "SCF damping must be in (0, 1]");
     if (o.max_iter <= 0) throw Fail(AXTB_ERR_INPUT, "the SCF needs at least 1 iteration");
     if (o.precision != 0 && o.precision != 1) throw Fail(AXTB_ERR_INPUT, "precision must be 0 (FP64) or 1 (split)");
-    if (o.mixer < 0 || o.mixer > 2) throw Fail(AXTB_ERR_INPUT, "unknown SCF mixer (0 auto, 1 Broyden, 2 DIIS)");
+    if (o.mixer < -1 || o.mixer > 2) throw Fail(AXTB_ERR_INPUT, "unknown SCF mixer (0 auto, 1 Broyden, 2 DIIS)");
+    if (o.conventions < 0 || o.conventions > 2) throw Fail(AXTB_ERR_INPUT, "unknown conventions (0 axtb, 1 xtb, 2 tblite)");
 }
 
 // ------------------------------------------------------------------ device arena
@@ -214,6 +277,8 @@ struct AxtbBatch {
     int nmol = 0, natT = 0, nshT = 0, naoT = 0;
     long long nnT = 0, npairT = 0, npdT = 0, nvecT = 0, nsqT = 0, ntiles = 0, nwk = 0, nhist = 0;
     int hist_cap = 0, nsp = 0;
+    int mixer_kind = 0;      // the mixer plan of the run: 0 auto, 1 Broyden, 2 DIIS
+    bool eeq_guess = true;   // the conventions start from EEQ charges
     axg::Batch B{};
     axg::State S{};
     axg::TeamPlan P{};
@@ -273,6 +338,9 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     mols = in;
     nmol = (int)mols.size();
     if (nmol <= 0) throw Fail(AXTB_ERR_INPUT, "empty batch");
+    const Conv cv(o.conventions);
+    mixer_kind = o.mixer < 0 ? cv.default_mixer : o.mixer;
+    eeq_guess = cv.eeq_guess;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
         throw Fail(AXTB_ERR_DEVICE, "no CUDA device: the GFN2-xTB engine has no CPU path");
@@ -364,10 +432,10 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
                 a_nsh[ia] = NSHELL[z - 1];
                 a_ao0[ia] = io;
                 a_sp[ia] = sp;
-                a_rcov[ia] = rcov_codata(z);
-                a_rad[ia] = ATOMIC_RAD_AA[z - 1] * AATOAU;
-                a_rcov_eeq[ia] = rcov_mctc(z);
-                a_en[ia] = PAULING_EN[z - 1];
+                a_rcov[ia] = cv.cn_rcov(z);
+                a_rad[ia] = cv.atomic_rad(z);
+                a_rcov_eeq[ia] = cv.eeq_rcov(z);
+                a_en[ia] = cv.en(z);
                 a_aes_rad[ia] = P_RAD[z - 1];
                 a_aes_vcn[ia] = P_VCN[z - 1];
                 a_dk[ia] = P_DKERNEL[z - 1];
@@ -433,8 +501,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         }
         sp_zeff[sp] = EFFECTIVE_NUCLEAR_CHARGE[z - 1];
         sp_gi[sp] = CHEMICAL_HARDNESS[z - 1] * 2.0;
-        sp_rcov[sp] = rcov_codata(z);
-        sp_en[sp] = PAULING_EN[z - 1];
+        sp_rcov[sp] = cv.d4_rcov(z);
+        sp_en[sp] = cv.d4_en(z);
         r4r2[sp] = std::sqrt(0.5 * (R4_OVER_R2[z - 1] * std::sqrt((double)z)));
         for (int ir = 0; ir < nr; ir++) {
             int s2 = REFSYS[z - 1][ir];
@@ -510,6 +578,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addI(nmol * 7);
     addL(nmol * 10);
     addD(nmol * 3);
+    addD(nmol);  // per-molecule pair cutoffs
     addI(natT * 6);
     addD(natT * 15);
     addI(nshT * 7);
@@ -637,8 +706,28 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.sp_c6ref = upD(c6ref);
     b.sp_rr = upD(sp_rr);
     b.sp_r0 = upD(sp_r0);
-    b.intcut = std::max(25.0 - 10.0 * std::log10(o.acc), 20.0);  // crates/axtb/src/basis.rs:135-137
-    b.kt = o.etemp * KB_HARTREE;
+    b.intcut = cv.intcut(o.acc);
+    // aufbau occupations up to the conventions' temperature (crates/axtb/src/xtb.rs:462)
+    b.kt = o.etemp <= cv.aufbau_max_etemp ? 0.0 : o.etemp * cv.kb;
+    b.cn_cut = cv.cn_cut;
+    b.rep_cut = cv.rep_cut;
+    b.d4_cn_cut = cv.d4_cn_cut;
+    b.d2_cut = cv.d2_cut;
+    b.d2_w = cv.d2_w;
+    b.d3_cut = cv.d3_cut;
+    b.d3_w = cv.d3_w;
+    b.eeq_cn_cut = cv.eeq_cn_cut;
+    b.eeq_cap = cv.eeq_cap;
+    b.output_aes = cv.output_aes ? 1 : 0;
+    {
+        vector<double> pc(nmol);
+        for (int m = 0; m < nmol; m++) {
+            double amin = INFINITY;
+            for (int i = 0; i < mols[m].nat; i++) amin = std::min(amin, a_amin[m_at0[m] + i]);
+            pc[m] = cv.pair_cut2(o.acc, amin);
+        }
+        b.m_paircut2 = upD(pc);
+    }
     b.damping = o.damping;
     b.econv = 1e-6 * o.acc;
     b.pconv = 2e-5 * o.acc;
@@ -1001,9 +1090,9 @@ void AxtbBatch::run(bool want_grad, bool warm) {
     for (int m = 0; m < nmol; m++) chol_flops += (1.0 / 3.0 + 2.0 / 3.0) * std::pow((double)mols[m].nao, 3.0);
     LAUNCH("team_overlap", chol_flops, 0,
            CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
-    bool eeq = opt.guess == 0 && !warm;
+    bool eeq = opt.guess == 0 && eeq_guess && !warm;
     if (warm) {
-        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, opt.mixer));
+        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind));
     } else if (eeq) {
         LAUNCH("eeq_matrix", 0, 0, k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT));
         ph = PH_EEQ;
@@ -1011,7 +1100,7 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
         LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     }
-    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, opt.mixer));
+    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind));
     // SCF: the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199): Broyden, then
     // for the molecules it left unconverged DIIS from the same start (auto); or one mixer alone
     auto scf_attempt = [&](bool diis) {
@@ -1035,8 +1124,8 @@ void AxtbBatch::run(bool want_grad, bool warm) {
             if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
         }
     };
-    scf_attempt(opt.mixer == 2);
-    if (opt.mixer == 0) {
+    scf_attempt(mixer_kind == 2);
+    if (mixer_kind == 0) {
         LAUNCH("restart_diis", 0, 0, k_restart_diis<<<nmol, T, 0, st>>>(B, S));
         CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -1047,6 +1136,9 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         ph = PH_WDENS;
         LAUNCH("team_wdens", w_flops(all), 0,
                CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+        if (B.output_aes)
+            LAUNCH("gradient_potentials", 0, 0,
+                   k_gradient_potentials_aes<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
         if (npairT > 0)
             LAUNCH("h0_gradient", 0, mat_bytes(all, 2.0),
                    k_h0_gradient<<<blocks_for(npairT, 128), 128, 0, st>>>(B, S, d_pair0, npairT, S.pair_buf));

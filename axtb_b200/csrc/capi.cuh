@@ -91,6 +91,7 @@ static Opt to_opt(const AxtbOptions* o) {
         r.precision = o->precision;
         r.device = o->device;
         r.mixer = o->mixer;
+        r.conventions = o->conventions;
     }
     return r;
 }
@@ -134,7 +135,8 @@ void axtb_gpu_default_options(AxtbOptions* o) {
     o->guess = 0;
     o->precision = 0;
     o->device = 0;
-    o->mixer = 0;
+    o->mixer = -1;
+    o->conventions = 0;
 }
 
 int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao) {

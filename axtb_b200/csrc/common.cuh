@@ -66,6 +66,12 @@ struct Batch {
     double damping;
     double econv, pconv;
     int max_iter;
+    // real-space cutoffs (bohr) of the conventions (crates/axtb/src/conventions.rs:150-353): GFN2
+    // CN, repulsion, D4 CN, D4 two-body and three-body with their smooth-switch widths, EEQ-guess
+    // CN with its log cap (<= 0: none); squared atom-pair cutoff of the integrals per molecule
+    double cn_cut, rep_cut, d4_cn_cut, d2_cut, d2_w, d3_cut, d3_w, eeq_cn_cut, eeq_cap;
+    const double* m_paircut2;
+    int output_aes;  // 1: gradient with the AES potentials of the output moments (xtb 6.8.0)
     int split;                        // 1: basis-transform and W GEMMs in split precision
 };
 

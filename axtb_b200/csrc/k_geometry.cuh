@@ -8,12 +8,7 @@
 
 namespace axg {
 
-// ---- constants of the axtb conventions (crates/axtb/src/conventions.rs:244-268) and models
-constexpr double CN_CUT = 40.0;       // GFN2 CN, conventions.rs:251
-constexpr double REP_CUT = 40.0;      // repulsion, conventions.rs:252
-constexpr double D4_CN_CUT = 40.0;    // D4 CN, conventions.rs:255
-constexpr double D2_CUT = 72.0, D2_W = 1.0, D3_CUT = 40.0, D3_W = 1.0;
-constexpr double EEQ_CN_CUT = 25.0;   // multicharge CN, crates/axtb/src/eeq.rs:27
+// ---- constants of the models; the real-space cutoffs of the conventions are Batch fields
 constexpr double D4_S6 = 1.0, D4_S8 = 2.7, D4_S9 = 5.0, D4_ALP = 16.0;  // crates/d4/src/disp.rs:24
 constexpr double D4_GA = 3.0, D4_WF = 6.0;  // crates/d4/src/model.rs:20-22
 
@@ -81,12 +76,12 @@ __global__ void k_cn(Batch B, State S) {
         double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
         if (r2 < 1e-12) continue;
         double r = sqrt(r2);
-        if (r2 <= CN_CUT * CN_CUT) c1 += dexp_count(r, B.a_rcov[a] + B.a_rcov[b]);
-        if (r2 <= D4_CN_CUT * D4_CN_CUT) {
+        if (r2 <= B.cn_cut * B.cn_cut) c1 += dexp_count(r, B.a_rcov[a] + B.a_rcov[b]);
+        if (r2 <= B.d4_cn_cut * B.d4_cn_cut) {
             int spb = B.a_sp[b];
             c2 += en_factor(B.sp_en[spa], B.sp_en[spb]) * erf_count(r, B.sp_rcov[spa] + B.sp_rcov[spb]);
         }
-        if (r2 <= EEQ_CN_CUT * EEQ_CN_CUT) c3 += erf_count(r, B.a_rcov_eeq[a] + B.a_rcov_eeq[b]);
+        if (r2 <= B.eeq_cn_cut * B.eeq_cn_cut) c3 += erf_count(r, B.a_rcov_eeq[a] + B.a_rcov_eeq[b]);
     }
     c1 = warp_sum(c1);
     c2 = warp_sum(c2);
@@ -94,8 +89,9 @@ __global__ void k_cn(Batch B, State S) {
     if (lane == 0) {
         S.cn[a] = c1;
         S.cn_d4[a] = c2;
-        const double cap = 8.0;  // multicharge log cap (crates/base/src/ncoord.rs log_cap)
-        S.cn_eeq[a] = log(1.0 + exp(cap)) - log(exp(cap - c3) + 1.0);
+        // multicharge's log cap (crates/base/src/ncoord.rs log_cap); none in the xtb conventions
+        const double cap = B.eeq_cap;
+        S.cn_eeq[a] = cap > 0.0 ? log(1.0 + exp(cap)) - log(exp(cap - c3) + 1.0) : c3;
     }
 }
 
@@ -129,7 +125,7 @@ __global__ void k_repulsion(Batch B, State S) {
         double v[3];
         dvec(S.xyz, a, b, v);
         double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-        if (r2 > REP_CUT * REP_CUT || r2 < 1e-12) continue;
+        if (r2 > B.rep_cut * B.rep_cut || r2 < 1e-12) continue;
         double r1 = sqrt(r2);
         double kexp = (za > 2 || B.a_Z[b] > 2) ? 1.5 : 1.0;
         double alpha = sqrt(B.a_rep_alpha[b] * B.a_rep_alpha[a]);
@@ -225,9 +221,9 @@ __device__ __forceinline__ void pair_c6(const Batch& B, const State& S, int a, i
 // two-body damped pair factor with its smooth switch (crates/d4/src/disp.rs:298-322):
 // pe (energy factor), pg (radial derivative / r); false outside the cutoff
 __device__ __forceinline__ bool d4_pair(const Batch& B, int spa, int spb, double r2, double& pe, double& pg) {
-    if (r2 > D2_CUT * D2_CUT || r2 < DBL_EPSILON) return false;
+    if (r2 > B.d2_cut * B.d2_cut || r2 < DBL_EPSILON) return false;
     double r = sqrt(r2), sw, dsw;
-    smooth_cut(r, D2_CUT, D2_W, sw, dsw);
+    smooth_cut(r, B.d2_cut, B.d2_w, sw, dsw);
     if (sw <= 0.0) return false;
     int k = spa * B.nsp + spb;
     double rr = B.sp_rr[k], r0 = B.sp_r0[k];
@@ -257,9 +253,9 @@ __global__ void k_atm_tables(Batch B, State S, double* wt, double* tt, const lon
         double v[3];
         dvec(S.xyz, a, k, v);
         double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-        if (r2 <= D3_CUT * D3_CUT && r2 >= DBL_EPSILON) {
+        if (r2 <= B.d3_cut * B.d3_cut && r2 >= DBL_EPSILON) {
             double r = sqrt(r2), sw, dsw;
-            smooth_cut(r, D3_CUT, D3_W, sw, dsw);
+            smooth_cut(r, B.d3_cut, B.d3_w, sw, dsw);
             double c6, da, db;
             pair_c6(B, S, a, k, c6, da, db);
             w = sqrt(fabs(c6)) * sw;
@@ -289,9 +285,9 @@ __global__ void k_atm(Batch B, State S, const double* wt, const double* tt, cons
         double vab[3];
         dvec(S.xyz, b, a, vab);  // R_b - R_a
         double r2 = vab[0] * vab[0] + vab[1] * vab[1] + vab[2] * vab[2];
-        if (r2 > D3_CUT * D3_CUT || r2 < DBL_EPSILON) continue;
+        if (r2 > B.d3_cut * B.d3_cut || r2 < DBL_EPSILON) continue;
         double r = sqrt(r2), sw, dsw;
-        smooth_cut(r, D3_CUT, D3_W, sw, dsw);
+        smooth_cut(r, B.d3_cut, B.d3_w, sw, dsw);
         if (sw <= 0.0) continue;
         double ir = 1.0 / r, t6 = 6.0 * T[(long long)la * n + lb];
         double r2_2 = r2 * r2;

@@ -221,7 +221,8 @@ __global__ void k_integrals(Batch B, State S, const long long* m_pd0, long long 
     dvec(S.xyz, ia, ja, vec);
     double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
     bool onsite = ia == ja;
-    if (!onsite && pair_screened(B.a_amin[ia], B.a_amin[ja], r2, B.intcut)) return;
+    // atom pairs beyond the conventions' distance cutoff (tblite) or screened by their exponents
+    if (!onsite && (r2 > B.m_paircut2[m] || pair_screened(B.a_amin[ia], B.a_amin[ja], r2, B.intcut))) return;
     double rr = onsite ? 0.0 : sqrt(sqrt(r2) / (B.a_rad[ja] + B.a_rad[ia]));
     double s[25], d[75], q[150];
     Shl ci, cj;
@@ -279,7 +280,7 @@ __global__ void k_h0_gradient(Batch B, State S, const long long* m_pair0, long l
     double vec[3];
     dvec(S.xyz, ia, ja, vec);
     double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
-    if (pair_screened(B.a_amin[ia], B.a_amin[ja], r2, B.intcut) || r2 < DBL_EPSILON) return;
+    if (r2 > B.m_paircut2[m] || pair_screened(B.a_amin[ia], B.a_amin[ja], r2, B.intcut) || r2 < DBL_EPSILON) return;
     double rr = sqrt(sqrt(r2) / (B.a_rad[ja] + B.a_rad[ia]));
     const double* vdi = S.vdp + 3 * ia;
     const double* vdj = S.vdp + 3 * ja;

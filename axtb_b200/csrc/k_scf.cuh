@@ -37,6 +37,28 @@ __device__ __forceinline__ void aes_g35(const State& S, int a, int b, double r2,
     g5 = gg5 * (1.0 / (1.0 + 6.0 * rr3 * rr));
 }
 
+// AES potential terms of partner b at atom a (crates/axtb/src/coulomb.rs:407-502) for the moments
+// (qat, dp, qp), w = R_a - R_b: added to the atom, dipole and quadrupole potentials of a
+__device__ __forceinline__ void aes_pair_potential(const State& S, int a, int b, const double* qat, const double* dp,
+                                                   const double* qp, const double w[3], double r2, double& va,
+                                                   double vd[3], double vq[6]) {
+    double g3, g5;
+    aes_g35(S, a, b, r2, g3, g5);
+    const double* mb = dp + 3 * b;
+    double qb = qat[b];
+    double mbw = mb[0] * w[0] + mb[1] * w[1] + mb[2] * w[2];
+    va += mbw * g3;
+    for (int k = 0; k < 3; k++) vd[k] += -w[k] * g3 * qb + g5 * (r2 * mb[k] - 3.0 * w[k] * mbw);
+    double tc[6] = {w[0] * w[0], w[0] * w[1], w[1] * w[1], w[0] * w[2], w[1] * w[2], w[2] * w[2]};
+    double thb = 0.0;
+    for (int k = 0; k < 6; k++) {
+        double t = QSCALE[k] * tc[k] * g5;
+        vq[k] += t * qb;
+        thb += t * qp[6 * b + k];
+    }
+    va += thb;
+}
+
 // potentials of the input moments: warp per atom (shell potentials of the atom's shells, atom,
 // dipole and quadrupole potentials); crates/axtb/src/xtb.rs:316-340 with coulomb.rs:407-502,
 // 1006-1021, 1141-1143 and crates/d4/src/disp.rs:420-455
@@ -62,21 +84,7 @@ __global__ void k_potentials(Batch B, State S) {
         double w[3];
         dvec(x, a, b, w);
         double r2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
-        double g3, g5;
-        aes_g35(S, a, b, r2, g3, g5);
-        const double* mb = S.dp_in + 3 * b;
-        double qb = S.qat_in[b];
-        double mbw = mb[0] * w[0] + mb[1] * w[1] + mb[2] * w[2];
-        va += mbw * g3;
-        for (int k = 0; k < 3; k++) vd[k] += -w[k] * g3 * qb + g5 * (r2 * mb[k] - 3.0 * w[k] * mbw);
-        double tc[6] = {w[0] * w[0], w[0] * w[1], w[1] * w[1], w[0] * w[2], w[1] * w[2], w[2] * w[2]};
-        double thb = 0.0;
-        for (int k = 0; k < 6; k++) {
-            double t = QSCALE[k] * tc[k] * g5;
-            vq[k] += t * qb;
-            thb += t * S.qp_in[6 * b + k];
-        }
-        va += thb;
+        aes_pair_potential(S, a, b, S.qat_in, S.dp_in, S.qp_in, w, r2, va, vd, vq);
         // D4: -dC6/dq_a * pair factor
         double pe, pg;
         if (d4_pair(B, spa, B.a_sp[b], r2, pe, pg)) {
@@ -92,6 +100,36 @@ __global__ void k_potentials(Batch B, State S) {
         S.vat[a] = va;
         for (int k = 0; k < 3; k++) S.vdp[3 * a + k] = vd[k] + 2.0 * B.a_dk[a] * S.dp_in[3 * a + k];
         for (int k = 0; k < 6; k++) S.vqp[6 * a + k] = vq[k] + 2.0 * B.a_qk[a] * S.qp_in[6 * a + k] * QSCALE[k];
+    }
+}
+
+// potentials of the gradient in the xtb 6.8.0 conventions (SccGradient::OutputAes,
+// crates/axtb/src/xtb.rs:700-722): the dipole and quadrupole potentials of the output moments,
+// and the atom potential of the last Fock matrix shifted by the AES atom potential of the output
+// moments minus that of the last input moments; warp per atom
+__global__ void k_gradient_potentials_aes(Batch B, State S) {
+    int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (a >= B.natT) return;
+    AtomView mv = mol_atoms(B, a);
+    const double* x = S.xyz;
+    double vo = 0.0, vi = 0.0, vd[3] = {0, 0, 0}, vq[6] = {0, 0, 0, 0, 0, 0};
+    double vdi[3] = {0, 0, 0}, vqi[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = mv.i0 + lane; b < mv.i0 + mv.n; b += 32) {
+        if (b == a) continue;
+        double w[3];
+        dvec(x, a, b, w);
+        double r2 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+        aes_pair_potential(S, a, b, S.qat_out, S.dp_out, S.qp_out, w, r2, vo, vd, vq);
+        aes_pair_potential(S, a, b, S.qat_in, S.dp_in, S.qp_in, w, r2, vi, vdi, vqi);
+    }
+    vo = warp_sum(vo);
+    vi = warp_sum(vi);
+    for (int k = 0; k < 3; k++) vd[k] = warp_sum(vd[k]);
+    for (int k = 0; k < 6; k++) vq[k] = warp_sum(vq[k]);
+    if (lane == 0) {
+        S.vat[a] += vo - vi;
+        for (int k = 0; k < 3; k++) S.vdp[3 * a + k] = vd[k] + 2.0 * B.a_dk[a] * S.dp_out[3 * a + k];
+        for (int k = 0; k < 6; k++) S.vqp[6 * a + k] = vq[k] + 2.0 * B.a_qk[a] * S.qp_out[6 * a + k] * QSCALE[k];
     }
 }
 
@@ -852,12 +890,12 @@ __global__ void k_cn_chain(Batch B, State S) {
         double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
         if (r2 < 1e-12) continue;
         double r = sqrt(r2);
-        if (r2 <= CN_CUT * CN_CUT) {
+        if (r2 <= B.cn_cut * B.cn_cut) {
             double d = dexp_dcount(r, B.a_rcov[a] + B.a_rcov[b]);
             double t = d * (S.dedcn[a] + S.dedcn[b]) / r;
             for (int k = 0; k < 3; k++) g[k] += t * v[k];
         }
-        if (r2 <= D4_CN_CUT * D4_CN_CUT) {
+        if (r2 <= B.d4_cn_cut * B.d4_cn_cut) {
             int spb = B.a_sp[b];
             double dc = en_factor(B.sp_en[spa], B.sp_en[spb]) * erf_dcount(r, B.sp_rcov[spa] + B.sp_rcov[spb]);
             double s = S.dedcn_d4[a] + S.dedcn_d4[b];

@@ -24,6 +24,7 @@ The output header is committed; the script only needs the axtb sources to regene
 """
 from __future__ import annotations
 
+import math
 import re
 import sys
 from pathlib import Path
@@ -32,6 +33,11 @@ REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
 OUT = Path(__file__).with_name("gfn2_tables.h")
 
 EVTOAU = 1.0 / 27.21138505
+# mctc-lib's Angstrom-to-bohr factor from CODATA 2018 (crates/base/src/units.rs:66-77), evaluated in
+# the same double-precision operations; xtb 6.8.0's tables are converted with it
+_HBAR_2018 = 6.62607015e-34 / (2.0 * math.pi)
+MCTC_AATOAU = 1.0 / (_HBAR_2018 / (9.1093837015e-31 * 299792458.0 * 7.2973525693e-3) * 1e10)
+NAMES = {"EVTOAU": EVTOAU, "XTB_AATOAU": MCTC_AATOAU}
 
 SOURCES = {
     "crates/axtb/src/param/gfn2_data.rs": [
@@ -47,6 +53,10 @@ SOURCES = {
     ],
     "crates/axtb/src/param/eeq_data.rs": ["EEQ_CHI", "EEQ_ETA", "EEQ_KCNCHI", "EEQ_RAD"],
     "crates/base/src/elements.rs": ["PAULING_EN", "COVALENT_RAD_2009_AA"],
+    # the xtb 6.8.0 program's element tables (its conventions row)
+    "crates/axtb/src/param/xtb_data.rs": [
+        "XTB_COVALENT_RAD_D3", "XTB_ATOMIC_RAD", "XTB_PAULING_EN", "XTB_D4_RCOV", "XTB_D4_EN",
+    ],
     "crates/d4/src/data.rs": [
         "CHEMICAL_HARDNESS", "EFFECTIVE_NUCLEAR_CHARGE", "R4_OVER_R2", "REFN", "REFQ_GFN2",
         "REFH_GFN2", "HCOUNT", "ASCALE", "REFCOVCN", "REFCN", "REFSYS", "ALPHAIW", "SSCALE",
@@ -82,7 +92,7 @@ def extract(text: str, name: str):
         rtype = m.group(2).strip()
         is_int = any(t in rtype for t in ("usize", "u8", "u32", "i32"))
         body = strip_comments(body)
-        value = eval(body, {"__builtins__": {}}, {"EVTOAU": EVTOAU})
+        value = eval(body, {"__builtins__": {}}, NAMES)
         return value, is_int
     raise KeyError(name)
 

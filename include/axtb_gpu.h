@@ -56,10 +56,16 @@ typedef struct AxtbOptions {
                           C, P, mixer and sums stay FP64. For SCC accuracy >= ~1e-3; tighter
                           settings ask for energy changes below its rounding floor. */
     int32_t device;    /* CUDA device ordinal; 0 */
-    int32_t mixer;     /* SCC mixer (crates/axtb/src/scf/mixing.rs:81-94 MixerKind): 0 auto (default:
-                          modified Broyden; a molecule it leaves unconverged, with a failed mixer or a
-                          lost Fermi level starts again from its start moments with DIIS and another
-                          max_iter iterations), 1 Broyden alone, 2 DIIS alone */
+    int32_t mixer;     /* SCC mixer (crates/axtb/src/scf/mixing.rs:81-94 MixerKind): -1 the
+                          conventions' (default: auto for axtb, Broyden for xtb and tblite); 0 auto
+                          (modified Broyden; a molecule it leaves unconverged, with a failed mixer or
+                          a lost Fermi level starts again from its start moments with DIIS and
+                          another max_iter iterations), 1 Broyden alone, 2 DIIS alone */
+    int32_t conventions; /* crates/axtb/src/conventions.rs Conventions: 0 axtb (default), 1 the xtb
+                          6.8.0 program's (its element tables, 25/30/50/25 bohr cutoffs, tblite's
+                          screening, aufbau up to 0.1 K, its EEQ-start CN, the gradient with the
+                          AES potentials of the output moments), 2 tblite 0.8.0's (mctc-lib radii,
+                          the same cutoffs, atom-pair integral cutoff, zero-charge start) */
 } AxtbOptions;
 
 /* Results of one single point (crates/base/src/method/results.rs:39-57). Array members are

@@ -70,6 +70,67 @@ double rcov_codata(int z) { return 4.0 / 3.0 * (COVALENT_RAD_2009_AA[z - 1] * AA
 double atomic_rad_codata(int z) { return ATOMIC_RAD_AA(z) * AATOAU; }
 // mctc-lib radii of the EEQ guess CN: crates/axtb/src/param/element_data.rs:15-24,94-103
 double rcov_mctc(int z) { return 4.0 / 3.0 * (MCTC_AATOAU * COVALENT_RAD_2009_AA[z - 1]); }
+// mctc-lib's atomic radii in bohr (tblite): crates/axtb/src/param/element_data.rs:26-58
+double atomic_rad_mctc(int z) { return MCTC_AATOAU * ATOMIC_RAD_AA(z); }
+
+// ---- conventions (crates/axtb/src/conventions.rs:150-353): the settings that differ between
+// axtb's default conventions, the xtb 6.8.0 program's and tblite 0.8.0's. Not restated: the
+// xtb 6.7.1 row; the per-triple ATM order and the full eigensolver of the program conventions
+// (the same numbers up to round-off as the pair sums and the occupied-only solve used here).
+const double KB_XTB_TBLITE = 3.166808578545117e-06;  // crates/base/src/units.rs:81
+struct Conv {
+    int id = 0;                    // 0 axtb, 1 xtb (6.8.0), 2 tblite (0.8.0)
+    double kb = KB_HARTREE;        // Boltzmann constant of the electronic temperature
+    double aufbau_max_etemp = 0.0; // up to this temperature (K) no Fermi smearing
+    bool eeq_guess = true;         // EEQ start (tblite: zero charges)
+    double eeq_cn_cut = 25.0, eeq_cap = 8.0;  // EEQ-guess CN cutoff; log cap (<= 0: none)
+    double cn_cut = 40.0, rep_cut = 40.0;     // GFN2 CN and repulsion cutoffs
+    double d4_cn_cut = 40.0, d2_cut = 72.0, d2_w = 1.0, d3_cut = 40.0, d3_w = 1.0;
+    bool output_aes = false;       // gradient with the AES potentials of the output moments
+    int default_mixer = 0;         // 0 auto, 1 Broyden
+};
+thread_local Conv g_conv;
+
+Conv make_conv(int id) {
+    Conv c;
+    c.id = id;
+    if (id == 0) return c;
+    // xtb 6.8.0 and tblite 0.8.0: conventions.rs:274-298 and 326-350
+    c.kb = KB_XTB_TBLITE;
+    c.cn_cut = c.rep_cut = 25.0;
+    c.d4_cn_cut = 30.0;  // RealspaceCutoff::TBLITE_GFN2, crates/d4/src/disp.rs:44-47
+    c.d2_cut = 50.0;
+    c.d3_cut = 25.0;
+    c.d2_w = c.d3_w = 0.05;
+    c.default_mixer = 1;
+    if (id == 1) {
+        c.aufbau_max_etemp = 0.1;
+        c.eeq_cn_cut = 40.0;  // the xtb program's guess CN: its D4 radii, 40 bohr, no cap
+        c.eeq_cap = 0.0;
+        c.output_aes = true;
+    } else {
+        c.eeq_guess = false;
+    }
+    return c;
+}
+// element tables of the conventions
+double conv_en(int z) { return g_conv.id == 1 ? XTB_PAULING_EN[z - 1] : PAULING_EN[z - 1]; }
+double conv_atomic_rad(int z) {
+    return g_conv.id == 1 ? XTB_ATOMIC_RAD[z - 1] : g_conv.id == 2 ? atomic_rad_mctc(z) : atomic_rad_codata(z);
+}
+double conv_cn_rcov(int z) {
+    return g_conv.id == 1 ? XTB_COVALENT_RAD_D3[z - 1] : g_conv.id == 2 ? rcov_mctc(z) : rcov_codata(z);
+}
+double conv_d4_rcov(int z) {
+    return g_conv.id == 1 ? XTB_D4_RCOV[z - 1] : g_conv.id == 2 ? rcov_mctc(z) : rcov_codata(z);
+}
+double conv_d4_en(int z) { return g_conv.id == 1 ? XTB_D4_EN[z - 1] : PAULING_EN[z - 1]; }
+double conv_eeq_rcov(int z) { return g_conv.id == 1 ? XTB_D4_RCOV[z - 1] : rcov_mctc(z); }
+// tblite's screening threshold (crates/axtb/src/basis.rs:140-143)
+double integral_cutoff_tblite(double acc) {
+    acc = std::min(std::max(acc, 1.0e-4), 1.0e3);
+    return std::min(std::max(25.0 - 10.0 * std::log10(acc), 5.0), 25.0);
+}
 
 
 inline double sq(double x) { return x * x; }
@@ -149,6 +210,7 @@ struct Basis {
     vector<int> sh2at, iao_sh, ish_at, nsh_at, iao_at, nao_at, ao2at, ao2sh;
     vector<double> amin_at;
     double intcut = 25.0;
+    double pair_cut2 = INFINITY;  // squared atom-pair distance cutoff of the integrals
 };
 
 // crates/axtb/src/gfn2.rs:34-56 and crates/axtb/src/basis.rs:165-229
@@ -178,8 +240,20 @@ Basis build_basis(const Mol& m, double acc) {
         b.nao_at.push_back(b.nao - b.iao_at[iat]);
         b.amin_at.push_back(amin);
     }
-    // xtb's primitive screening threshold: crates/axtb/src/basis.rs:135-137
-    b.intcut = std::max(25.0 - 10.0 * std::log10(acc), 20.0);
+    // primitive screening (crates/axtb/src/gfn2.rs:58-62): axtb the xtb program's threshold
+    // (crates/axtb/src/basis.rs:135-137), xtb 6.8.0 tblite's at the SCF accuracy, tblite tblite's at
+    // accuracy 1; tblite also leaves out atom pairs beyond sqrt(2 cut(acc) / min alpha), at most
+    // 40 bohr (crates/axtb/src/basis.rs:247-249)
+    if (g_conv.id == 0) b.intcut = std::max(25.0 - 10.0 * std::log10(acc), 20.0);
+    else if (g_conv.id == 1) b.intcut = integral_cutoff_tblite(acc);
+    else b.intcut = integral_cutoff_tblite(1.0);
+    b.pair_cut2 = INFINITY;
+    if (g_conv.id == 2) {
+        double amin = INFINITY;
+        for (double a : b.amin_at) amin = std::min(amin, a);
+        double pc = std::min(std::sqrt(2.0 * integral_cutoff_tblite(acc) / amin), 40.0);
+        b.pair_cut2 = pc * pc;
+    }
     return b;
 }
 
@@ -472,7 +546,7 @@ double kshell(int k, int l) {
 
 // hscale[jsp][isp][jsh][ish] of crates/axtb/src/gfn2.rs:73-89 for bra shell (zj, jsh), ket (zi, ish)
 double hscale(int zj, int jsh, int zi, int ish) {
-    double den = sq(PAULING_EN[zj - 1] - PAULING_EN[zi - 1]);
+    double den = sq(conv_en(zj) - conv_en(zi));
     int jl = ANG_SHELL[zj - 1][jsh], il = ANG_SHELL[zi - 1][ish];
     double za = SLATER_EXPONENT[zj - 1][jsh], zb = SLATER_EXPONENT[zi - 1][ish];
     double zij = std::pow(2.0 * std::sqrt(za * zb) / (za + zb), 0.5);
@@ -498,8 +572,8 @@ Model build_model(const Mol& m, double acc) {
     }
     for (int i = 0; i < m.nat; i++) {
         int z = m.Z[i];
-        md.rad.push_back(atomic_rad_codata(z));
-        md.cn_rcov.push_back(rcov_codata(z));
+        md.rad.push_back(conv_atomic_rad(z));
+        md.cn_rcov.push_back(conv_cn_rcov(z));
         md.dkernel.push_back(P_DKERNEL[z - 1]);
         md.qkernel.push_back(P_QKERNEL[z - 1]);
         md.aes_rad.push_back(P_RAD[z - 1]);
@@ -522,7 +596,7 @@ double dexp_dcount(double r, double rc) {
     return exp_dcount(10.0, r, rc) * exp_count(20.0, r, rc + 2.0) + exp_count(10.0, r, rc) * exp_dcount(20.0, r, rc + 2.0);
 }
 
-const double CN_CUTOFF = 40.0;  // conventions.rs:251
+#define CN_CUTOFF (g_conv.cn_cut)  // conventions.rs:251, 285, 339
 
 vector<double> gfn2_cn(const Model& md) {
     const Mol& m = md.m;
@@ -582,7 +656,7 @@ Ints build_ints(const Model& md, const vector<double>& se) {
             double vec[3] = {m.R(iat)[0] - m.R(jat)[0], m.R(iat)[1] - m.R(jat)[1], m.R(iat)[2] - m.R(jat)[2]};
             double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
             bool onsite = iat == jat;
-            if (!onsite && pair_screened(b.amin_at[iat], b.amin_at[jat], r2, b.intcut)) continue;
+            if (!onsite && (r2 > b.pair_cut2 || pair_screened(b.amin_at[iat], b.amin_at[jat], r2, b.intcut))) continue;
             double rr = onsite ? 0.0 : std::sqrt(std::sqrt(r2) / (md.rad[jat] + md.rad[iat]));
             for (int ish = 0; ish < b.nsh_at[iat]; ish++) {
                 int si = b.ish_at[iat] + ish;
@@ -826,7 +900,7 @@ void aes_grad(const Model& md, const AesCache& c, const vector<double>& qat, con
 double repulsion(const Model& md, vector<double>* g) {
     const Mol& m = md.m;
     double e = 0.0;
-    const double cutoff = 40.0;
+    const double cutoff = g_conv.rep_cut;
     for (int i = 0; i < m.nat; i++)
         for (int j = 0; j < i; j++) {
             double v[3] = {m.R(i)[0] - m.R(j)[0], m.R(i)[1] - m.R(j)[1], m.R(i)[2] - m.R(j)[2]};
@@ -860,7 +934,11 @@ double repulsion(const Model& md, vector<double>* g) {
 const int MAXREF = 7, NFREQ = 23;
 const double D4_GA = 3.0, D4_GC = 2.0, D4_WF = 6.0;
 const double S6 = 1.0, S8 = 2.7, S9 = 5.0, A1 = 0.52, A2 = 5.0, ALP = 16.0;
-const double D4_CN_CUT = 40.0, D2_CUT = 72.0, D2_W = 1.0, D3_CUT = 40.0, D3_W = 1.0;
+#define D4_CN_CUT (g_conv.d4_cn_cut)
+#define D2_CUT (g_conv.d2_cut)
+#define D2_W (g_conv.d2_w)
+#define D3_CUT (g_conv.d3_cut)
+#define D3_W (g_conv.d3_w)
 
 double zeta_f(double a, double c, double qref, double qmod) {
     if (qmod < 0.0) return std::exp(a);
@@ -973,8 +1051,8 @@ D4 d4_setup(const Mol& m) {
         d.zeff.push_back(EFFECTIVE_NUCLEAR_CHARGE[z - 1]);
         d.eta.push_back(CHEMICAL_HARDNESS[z - 1]);
         d.r4r2.push_back(std::sqrt(0.5 * (R4_OVER_R2[z - 1] * std::sqrt((double)z))));
-        d.rcov.push_back(rcov_codata(z));
-        d.en.push_back(PAULING_EN[z - 1]);
+        d.rcov.push_back(conv_d4_rcov(z));
+        d.en.push_back(conv_d4_en(z));
     }
     // reference polarisabilities and C6 table
     vector<double> aiw((size_t)d.nsp * MAXREF * NFREQ, 0.0);
@@ -1260,13 +1338,14 @@ vector<double> eeq_charges(const Mol& m) {
         for (int j = 0; j < i; j++) {
             double v[3] = {m.R(i)[0] - m.R(j)[0], m.R(i)[1] - m.R(j)[1], m.R(i)[2] - m.R(j)[2]};
             double r2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-            if (r2 > 25.0 * 25.0 || r2 < 1e-12) continue;
-            double c = erf_count(std::sqrt(r2), rcov_mctc(m.Z[i]) + rcov_mctc(m.Z[j]));
+            if (r2 > g_conv.eeq_cn_cut * g_conv.eeq_cn_cut || r2 < 1e-12) continue;
+            double c = erf_count(std::sqrt(r2), conv_eeq_rcov(m.Z[i]) + conv_eeq_rcov(m.Z[j]));
             cn[i] += c;
             cn[j] += c;
         }
-    const double cap = 8.0;
-    for (double& c : cn) c = std::log(1.0 + std::exp(cap)) - std::log(std::exp(cap - c) + 1.0);
+    const double cap = g_conv.eeq_cap;
+    if (cap > 0.0)
+        for (double& c : cn) c = std::log(1.0 + std::exp(cap)) - std::log(std::exp(cap - c) + 1.0);
     int N = n + 1;
     vector<double> A((size_t)N * N, 0.0), x(N);
     double sqrt2pi = std::sqrt(2.0 / PI);
@@ -1867,7 +1946,10 @@ int run(OracleRun* R) {
     }
     double acc = R->accuracy;
     if (!(acc > 0.0)) throw Fail(1, "accuracy must be positive");
-    if (R->mixer < 0 || R->mixer > 2) throw Fail(1, "unknown SCF mixer (auto, broyden or diis)");
+    if (R->conventions < 0 || R->conventions > 2) throw Fail(1, "unknown conventions (axtb, xtb or tblite)");
+    g_conv = make_conv(R->conventions);
+    int mixer_kind = R->mixer < 0 ? g_conv.default_mixer : R->mixer;
+    if (mixer_kind > 2) throw Fail(1, "unknown SCF mixer (auto, broyden or diis)");
     Model md = build_model(m, acc);
     const Basis& b = md.b;
     int nat = m.nat, nsh = b.nsh, nao = b.nao;
@@ -1883,7 +1965,8 @@ int run(OracleRun* R) {
     if (nocc < 0.0 || nuhf > nocc) throw Fail(1, "impossible electron count");
     double nalpha = (nocc + nuhf) / 2.0, nbeta = (nocc - nuhf) / 2.0;
     if (nalpha > nao + 1e-9) throw Fail(1, "too many electrons for the basis");
-    double kt = R->etemp * KB_HARTREE;
+    // aufbau occupations up to the conventions' temperature (crates/axtb/src/xtb.rs:462)
+    double kt = R->etemp <= g_conv.aufbau_max_etemp ? 0.0 : R->etemp * g_conv.kb;
 
     // geometry: CN, self energies, gamma, AES cache, D4 (crates/axtb/src/xtb.rs:275-292)
     vector<double> cn = gfn2_cn(md);
@@ -1909,7 +1992,7 @@ int run(OracleRun* R) {
     st.qsh.assign(nsh, 0.0);
     st.dp.assign(3 * nat, 0.0);
     st.qp.assign(6 * nat, 0.0);
-    {
+    if (g_conv.eeq_guess) {
         vector<double> q = eeq_charges(m);
         for (int iat = 0; iat < nat; iat++) {
             int is = b.ish_at[iat], ns = b.nsh_at[iat];
@@ -1930,14 +2013,14 @@ int run(OracleRun* R) {
     Moments out;
     bool converged = false;
     int iters = 0, iters_all = 0;
-    vector<double> packed;
+    vector<double> packed, q_last;  // q_last: the last input of the last attempt
     // the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199, run by
     // crates/axtb/src/xtb.rs:590-645): auto = Broyden, then DIIS from the start guess with its own
     // max_iter; a failed mixer or a lost Fermi level gives way to the next attempt and ends the
     // last one with its error (non-finite values end the single point at once)
     const int plan_auto[2] = {1, 2}, plan_broyden[1] = {1}, plan_diis[1] = {2};
-    const int* plan = R->mixer == 1 ? plan_broyden : R->mixer == 2 ? plan_diis : plan_auto;
-    int nplan = R->mixer == 0 ? 2 : 1;
+    const int* plan = mixer_kind == 1 ? plan_broyden : mixer_kind == 2 ? plan_diis : plan_auto;
+    int nplan = mixer_kind == 0 ? 2 : 1;
     for (int ia = 0; ia < nplan && !converged; ia++) {
         bool last_attempt = ia + 1 == nplan;
         std::unique_ptr<VMix> mixer;
@@ -2074,7 +2157,8 @@ int run(OracleRun* R) {
             }
         }
         iters_all += iters;
-        R->mixer_used = plan[ia] == 1 ? 0 : (R->mixer == 0 ? 2 : 1);
+        R->mixer_used = plan[ia] == 1 ? 0 : (mixer_kind == 0 ? 2 : 1);
+        q_last = mix.q_in;
     }
     // iterations of the converged attempt; of all attempts when none converged (xtb.rs:624-645)
     R->iterations = converged ? iters : iters_all;
@@ -2114,7 +2198,21 @@ int run(OracleRun* R) {
     if (!converged) throw Fail(3, "SCF not converged");
     if (wantg) {
         // add_scc_gradient (crates/axtb/src/xtb.rs:346-387) with the output moments and the
-        // potentials of the last Fock matrix (SccGradient::Output)
+        // potentials of the last Fock matrix (SccGradient::Output); the xtb 6.8.0 conventions take
+        // the dipole and quadrupole potentials of the output moments and shift the atom potential
+        // by the AES atom potential of the output moments minus that of the last input
+        // (SccGradient::OutputAes, crates/axtb/src/xtb.rs:700-722)
+        if (g_conv.output_aes) {
+            Moments in;
+            unpack(q_last, b, nat, in);
+            vector<double> ai(nat, 0.0), di(3 * nat, 0.0), qi(6 * nat, 0.0);
+            vector<double> ao(nat, 0.0), dout(3 * nat, 0.0), qout(6 * nat, 0.0);
+            aes_potential(md, ac, in.qat, in.dp, in.qp, ai, di, qi);
+            aes_potential(md, ac, out.qat, out.dp, out.qp, ao, dout, qout);
+            pot.vdp = dout;
+            pot.vqp = qout;
+            for (int i = 0; i < nat; i++) pot.vat[i] += ao[i] - ai[i];
+        }
         es2_grad(md, out.qsh, grad);
         aes_grad(md, ac, out.qat, out.dp, out.qp, grad, dedcn);
         d4_grad(d4, m, out.qat, grad);
@@ -2128,7 +2226,7 @@ int run(OracleRun* R) {
                 int zj = m.Z[jat];
                 double vec[3] = {m.R(iat)[0] - m.R(jat)[0], m.R(iat)[1] - m.R(jat)[1], m.R(iat)[2] - m.R(jat)[2]};
                 double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
-                if (pair_screened(b.amin_at[iat], b.amin_at[jat], r2, b.intcut)) continue;
+                if (r2 > b.pair_cut2 || pair_screened(b.amin_at[iat], b.amin_at[jat], r2, b.intcut)) continue;
                 if (r2 < DBL_EPSILON) continue;
                 double rr = std::sqrt(std::sqrt(r2) / (md.rad[jat] + md.rad[iat]));
                 double dg[3] = {0, 0, 0}, dcni = 0.0, dcnj = 0.0;
@@ -2249,6 +2347,7 @@ extern "C" int oracle_diis_linear(int n, const double* eig, const double* b, dou
 extern "C" int oracle_integrals(int nat, const int* numbers, const double* positions, double acc, double* cn_out,
                                 double* S, double* H0, double* D, double* Q) {
     try {
+        g_conv = make_conv(0);
         Mol m;
         m.nat = nat;
         m.Z.assign(numbers, numbers + nat);

@@ -1,7 +1,7 @@
 /* TEST INFRASTRUCTURE - NOT PART OF THE PRODUCT.
  *
- * CPU FP64 restatement of axtb's GFN2-xTB energy + analytic gradient single point in the
- * default ("axtb") conventions, used only as the parity checker of the CUDA path (tests/,
+ * CPU FP64 restatement of axtb's GFN2-xTB energy + analytic gradient single point in its
+ * default ("axtb") conventions and its xtb 6.8.0 and tblite 0.8.0 conventions, used only as the parity checker of the CUDA path (tests/,
  * __graft_entry__.smoke) and as the timed CPU baseline of bench.py. Parity of this restatement
  * is pinned against the reference's own recorded results (tests/golden, generated from
  * axtb tests/reference_matrix/results.json: absolute energies, energy terms, charges and
@@ -27,7 +27,9 @@ typedef struct {
     int want_gradient;
     int eig_backend;         /* 0: builtin Householder/QL, 1: dlopen'ed LAPACK when found */
     int lapack_threads;      /* threads of the LAPACK backend (0 = library default) */
-    int mixer;               /* 0: auto (Broyden, then DIIS from the start guess), 1: Broyden, 2: DIIS */
+    int mixer;               /* -1: the conventions' mixer; 0: auto (Broyden, then DIIS from the
+                                start guess), 1: Broyden, 2: DIIS */
+    int conventions;         /* 0: axtb (default), 1: the xtb 6.8.0 program's, 2: tblite 0.8.0's */
     /* outputs (caller-allocated; any may be NULL) */
     double* energy;
     double* gradient;        /* nat*3 */

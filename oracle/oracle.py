@@ -23,7 +23,7 @@ class _Run(C.Structure):
         ("nat", C.c_int), ("numbers", C.POINTER(C.c_int)), ("positions", C.POINTER(C.c_double)),
         ("charge", C.c_double), ("uhf", C.c_int), ("accuracy", C.c_double), ("etemp", C.c_double),
         ("max_iter", C.c_int), ("want_gradient", C.c_int), ("eig_backend", C.c_int),
-        ("lapack_threads", C.c_int), ("mixer", C.c_int),
+        ("lapack_threads", C.c_int), ("mixer", C.c_int), ("conventions", C.c_int),
         ("energy", C.POINTER(C.c_double)), ("gradient", C.POINTER(C.c_double)),
         ("qat", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)),
         ("dpat", C.POINTER(C.c_double)), ("qpat", C.POINTER(C.c_double)),
@@ -36,7 +36,8 @@ class _Run(C.Structure):
     ]
 
 
-MIXERS = {"auto": 0, "broyden": 1, "diis": 2}
+MIXERS = {None: -1, "auto": 0, "broyden": 1, "diis": 2}
+CONVENTIONS = {"axtb": 0, "xtb": 1, "tblite": 2}
 MIXER_USED = ("broyden", "diis", "diis-fallback")
 
 TERM_NAMES = ("repulsion", "dispersion", "electronic", "isotropic_es", "third_order", "anisotropic",
@@ -100,10 +101,13 @@ def sizes(numbers):
 
 
 def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=300.0, max_iter=250,
-                gradient=True, matrices=False, lapack=False, lapack_threads=1, mixer="auto", failed=False):
+                gradient=True, matrices=False, lapack=False, lapack_threads=1, mixer=None, failed=False,
+                conventions="axtb"):
     """Run the oracle; returns a dict (energy, gradient, qat, qsh, dpat, qpat, dipole, terms, emo,
-    focc, iterations, converged, mixer_used[, density, wdensity]). ``mixer``: "auto" (Broyden,
-    then DIIS from the start guess), "broyden" or "diis". Raises RuntimeError on a failed SCF
+    focc, iterations, converged, mixer_used[, density, wdensity]). ``mixer``: None (the
+    conventions' mixer: auto for axtb, Broyden for xtb and tblite), "auto" (Broyden, then DIIS
+    from the start guess), "broyden" or "diis"; ``conventions``: "axtb", "xtb" (6.8.0) or
+    "tblite" (0.8.0). Raises RuntimeError on a failed SCF
     unless ``failed`` (then the dict of the failed run carries ``status`` and ``error``)."""
     z = np.ascontiguousarray(numbers, dtype=np.int32)
     x = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
@@ -130,6 +134,7 @@ def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=30
     r.eig_backend = 1 if lapack else 0
     r.lapack_threads = int(lapack_threads)
     r.mixer = MIXERS[mixer]
+    r.conventions = CONVENTIONS[conventions]
     for k in ("energy", "gradient", "qat", "qsh", "dpat", "qpat", "dipole", "terms", "emo", "focc"):
         setattr(r, k, _p(out[k]))
     if matrices:

@@ -12,7 +12,9 @@ structures, multielement, charges, spin, etemp_acc, open_shell_metals, threads) 
     tests/golden/reference_matrix.json
 
 with numbers, positions (bohr), charge, uhf, accuracy, etemp, max_iter and the recorded axtb
-results. Run once in a checkout that has the axtb sources::
+results, plus axtb's energies and iterations in its xtb (6.8.0) and tblite (0.8.0) conventions
+(``programs["axtb[xtb]"]``, ``programs["axtb[tblite]"]``). Run once in a checkout that has the
+axtb sources::
 
     python tests/golden/make_golden.py [path-to-axtb-checkout]
 """
@@ -58,6 +60,11 @@ def main() -> None:
                 "charges": ax.get("charges"),
                 "dipole": ax.get("dipole"),
                 "iterations": ax.get("iterations"),
+                # axtb 0.1.0 in its xtb (6.8.0) and tblite (0.8.0) conventions, where it ran
+                "conventions": {k: {"energy": r["programs"][p]["energy"],
+                                    "iterations": r["programs"][p].get("iterations")}
+                                for k, p in (("xtb", "axtb[xtb]"), ("tblite", "axtb[tblite]"))
+                                if r["programs"].get(p, {}).get("ok") and "energy" in r["programs"][p]},
             })
     OUT.write_text(json.dumps({"source": "axtb tests/reference_matrix/results.json (programs.axtb)",
                                "cases": out}, indent=0))
