@@ -65,6 +65,7 @@ SIGNATURES = {
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "axtb_gpu_batch_debug": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, PD]),
     "axtb_gpu_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "axtb_gpu_batch_set_restart": (C.c_int, [C.c_void_p, C.c_int32]),
     "axtb_gpu_batch_profile": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
 }
 

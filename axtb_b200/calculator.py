@@ -213,6 +213,14 @@ class Batch:
             raise AxtbError(rc, _lib.last_error(None))
         return st
 
+    def set_restart(self, enable: bool = True):
+        """Start later runs from each molecule's converged moments of the previous run (a
+        trajectory of geometries); a molecule that then does not converge runs once more from
+        the guess (axtb's Calculator under Restart::Previous)."""
+        rc = _lib.load().axtb_gpu_batch_set_restart(self._b, int(bool(enable)))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+
     def set_profiling(self, enable: bool = True):
         _lib.load().axtb_gpu_batch_set_profiling(self._b, int(bool(enable)))
 

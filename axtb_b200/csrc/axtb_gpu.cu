@@ -278,6 +278,7 @@ struct AxtbBatch {
     long long nnT = 0, npairT = 0, npdT = 0, nvecT = 0, nsqT = 0, ntiles = 0, nwk = 0, nhist = 0;
     int hist_cap = 0, nsp = 0;
     int mixer_kind = 0;      // the mixer plan of the run: 0 auto, 1 Broyden, 2 DIIS
+    bool restart = false;    // molecules start from their previous converged moments
     bool eeq_guess = true;   // the conventions start from EEQ charges
     axg::Batch B{};
     axg::State S{};
@@ -595,6 +596,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addI(nmol * 7);
     addI(nmol);
     addI(nmol);
+    addI(nmol);
+    addI(nmol);
     addD((size_t)nmol * 8);                          // DIIS scalars
     addD((size_t)nshT + (size_t)natT * 10);          // start moments
     addD((size_t)nshT * 3 + (size_t)natT * 2 + (size_t)natT * 6 + (size_t)natT * 12 + (size_t)nshT + natT * 10);
@@ -771,6 +774,9 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.iter = ar.take<int>(nmol);
     s.mix_used = ar.take<int>(nmol);
     s.niter_prev = ar.take<int>(nmol);
+    s.have_guess = ar.take<int>(nmol);
+    s.retry = ar.take<int>(nmol);
+    CK(cudaMemsetAsync(s.have_guess, 0, sizeof(int) * nmol, st));
     s.diis = ar.take<double>((size_t)nmol * 8);
     s.start = ar.take<double>((size_t)nshT + (size_t)natT * 10);
     s.qsh_in = ar.take<double>(nshT);
@@ -876,9 +882,10 @@ __device__ void begin_attempts(const Batch& B, const State& S, int m, int mixer)
 
 // start moments: EEQ charges split over the shells by reference occupation
 // (crates/axtb/src/xtb.rs:522-549), zero multipoles, packed SCC vector
-__global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq, int mixer) {
+__global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq, int mixer, const int* only) {
     int m = blockIdx.x;
-    if (m >= B.nmol) return;
+    if (m >= B.nmol || (only && !only[m])) return;
+    if (only && threadIdx.x == 0) S.status[m] = 0;  // a fresh retry forgets the failed attempt
     int a0 = B.m_at0[m], nat = B.m_nat[m];
     for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
         double tot = 0.0;
@@ -897,10 +904,11 @@ __global__ void k_start(Batch B, State S, const double* qeeq, int use_eeq, int m
     begin_attempts(B, S, m, mixer);
 }
 
-// start of a warm SCF: the previous converged output moments of every molecule
-__global__ void k_start_warm(Batch B, State S, int mixer) {
+// start of a warm SCF: the previous converged output moments of every molecule (of those with
+// only[m] set)
+__global__ void k_start_warm(Batch B, State S, int mixer, const int* only) {
     int m = blockIdx.x;
-    if (m >= B.nmol) return;
+    if (m >= B.nmol || (only && !only[m])) return;
     int a0 = B.m_at0[m], nat = B.m_nat[m], s0 = B.m_sh0[m], nsh = B.m_nsh[m];
     for (int s = s0 + threadIdx.x; s < s0 + nsh; s += blockDim.x) S.qsh_in[s] = S.qsh_out[s];
     for (int a = a0 + threadIdx.x; a < a0 + nat; a += blockDim.x) {
@@ -927,7 +935,7 @@ __global__ void k_restart_diis(Batch B, State S) {
         int st = S.status[m];
         bool hard = (st & (ST_NOT_PD | ST_FOCK | ST_TIMEOUT)) != 0 ||
                     (!(st & ST_FERMI) && (st & (ST_NONFINITE | ST_INVIT)) != 0);
-        s_go = !S.conv[m] && !hard;
+        s_go = !S.conv[m] && !hard && S.mix_used[m] == 0;  // a Broyden attempt that just ended
     }
     __syncthreads();
     if (!s_go) return;
@@ -954,6 +962,15 @@ __global__ void k_restart_diis(Batch B, State S) {
         diis_reset(B, S, m);
         S.active[m] = 1;
     }
+}
+
+// molecules that started from their previous moments and ended unconverged run once more from
+// the fresh guess (crates/axtb/src/calculator.rs:194-206, RetryLadder::warm_then_fresh, which
+// climbs on ScfNotConverged only: crates/base/src/method/retry.rs:119-158)
+__global__ void k_fresh_mask(Batch B, State S) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= B.nmol) return;
+    S.retry[m] = S.have_guess[m] && !S.conv[m] && (S.status[m] & ~ST_HISTORY) == 0;
 }
 
 }  // namespace axg
@@ -1092,7 +1109,7 @@ void AxtbBatch::run(bool want_grad, bool warm) {
            CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     bool eeq = opt.guess == 0 && eeq_guess && !warm;
     if (warm) {
-        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind));
+        LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind, nullptr));
     } else if (eeq) {
         LAUNCH("eeq_matrix", 0, 0, k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT));
         ph = PH_EEQ;
@@ -1100,7 +1117,10 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
         LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
     }
-    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind));
+    if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind, nullptr));
+    // restarts: a molecule with converged moments from the previous run starts from them
+    if (restart && !warm)
+        LAUNCH("start_warm", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind, S.have_guess));
     // SCF: the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199): Broyden, then
     // for the molecules it left unconverged DIIS from the same start (auto); or one mixer alone
     auto scf_attempt = [&](bool diis) {
@@ -1124,13 +1144,31 @@ void AxtbBatch::run(bool want_grad, bool warm) {
             if (std::none_of(act.begin(), act.end(), [](int v) { return v != 0; })) break;
         }
     };
-    scf_attempt(mixer_kind == 2);
-    if (mixer_kind == 0) {
-        LAUNCH("restart_diis", 0, 0, k_restart_diis<<<nmol, T, 0, st>>>(B, S));
-        CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+    auto scf_plan = [&]() {
+        scf_attempt(mixer_kind == 2);
+        if (mixer_kind == 0) {
+            LAUNCH("restart_diis", 0, 0, k_restart_diis<<<nmol, T, 0, st>>>(B, S));
+            CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::copy(h_act, h_act + nmol, act.begin());
+            if (std::any_of(act.begin(), act.end(), [](int v) { return v != 0; })) scf_attempt(true);
+        }
+    };
+    scf_plan();
+    if (restart && !warm) {
+        // warm starts that did not converge: the whole plan once more from the fresh guess
+        LAUNCH("fresh_mask", 0, 0, k_fresh_mask<<<blocks_for(nmol, T), T, 0, st>>>(B, S));
+        CK(cudaMemcpyAsync(h_act, S.retry, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        std::copy(h_act, h_act + nmol, act.begin());
-        if (std::any_of(act.begin(), act.end(), [](int v) { return v != 0; })) scf_attempt(true);
+        if (std::any_of(h_act, h_act + nmol, [](int v) { return v != 0; })) {
+            LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind, S.retry));
+            CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            std::copy(h_act, h_act + nmol, act.begin());
+            scf_plan();
+        }
+        // the converged moments are the next run's starts
+        CK(cudaMemcpyAsync(S.have_guess, S.conv, sizeof(int) * nmol, cudaMemcpyDeviceToDevice, st));
     }
     if (want_grad) {
         ph = PH_WDENS;

@@ -193,12 +193,13 @@ int axtb_gpu_singlepoint(AxtbHandle* h, const double* positions, int32_t want_gr
         b.mols[0].xyz = m.xyz;
         b.upload_positions(m.xyz.data(), false);
         int32_t st = 0;
-        // warm start from the previous geometry's moments, then once more from the guess
-        // (crates/axtb/src/calculator.rs:194-206)
+        // warm start from the previous geometry's moments, then once more from the guess when
+        // that did not converge (crates/axtb/src/calculator.rs:194-206; the ladder climbs on
+        // ScfNotConverged only, crates/base/src/method/retry.rs:119-158)
         bool warm = h->have_guess;
         b.run(want_gradient != 0, warm);
         b.extract(out, &st, want_gradient != 0);
-        if (st != AXTB_OK && warm) {
+        if (st == AXTB_ERR_SCF_NOT_CONVERGED && warm) {
             b.run(want_gradient != 0, false);
             b.extract(out, &st, want_gradient != 0);
         }
@@ -310,6 +311,15 @@ int axtb_gpu_batch(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, i
 }
 
 // ---- introspection (include/axtb_gpu_debug.h)
+int axtb_gpu_batch_set_restart(AxtbBatch* b, int32_t enable) {
+    if (!b) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        b->restart = enable != 0;
+        CK(cudaMemsetAsync(b->S.have_guess, 0, sizeof(int) * b->nmol, b->st));
+        CK(cudaStreamSynchronize(b->st));
+    });
+}
+
 int axtb_gpu_batch_set_profiling(AxtbBatch* b, int32_t enable) {
     if (!b) return AXTB_ERR_INPUT;
     b->profiling = enable != 0;

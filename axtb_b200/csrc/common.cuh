@@ -102,6 +102,8 @@ struct State {
     double* start;                  // nshT + 10 natT: start moments (qsh; qat, dp, qp per atom)
     int* mix_used;                  // nmol: 0 Broyden, 1 DIIS, 2 DIIS after Broyden
     int* niter_prev;                // nmol: iterations of an earlier attempt
+    int* have_guess;                // nmol: 1 when the molecule's output moments are a converged start
+    int* retry;                     // nmol: molecules that run again from the fresh guess
     // per molecule scalars
     double *energy, *elast, *de, *res, *ts, *e_fixed;  // nmol
     double* terms;     // nmol*8

@@ -139,6 +139,12 @@ int axtb_gpu_batch_run(AxtbBatch* b, const double* positions, int32_t want_gradi
                        int32_t* status);
 int axtb_gpu_batch_run_device(AxtbBatch* b, const double* d_positions, int32_t want_gradient, double* d_energy,
                               double* d_gradient, int32_t* status);
+/* Restarts across runs (a trajectory of geometries): with enable = 1, every later run starts
+ * each molecule from its converged moments of the previous run (a molecule without them from
+ * the guess), and a molecule that then ends unconverged runs once more from the guess, as each
+ * molecule's axtb::Calculator does under Restart::Previous (crates/axtb/src/calculator.rs:185-206,
+ * crates/base/src/method/retry.rs:150-158). enable = 0 (the default) forgets the moments. */
+int axtb_gpu_batch_set_restart(AxtbBatch* b, int32_t enable);
 /* The CUDA stream (cudaStream_t) the batch runs on, for callers that time or order work. */
 void* axtb_gpu_batch_stream(AxtbBatch* b);
 /* Number of kernels the last run launched (counted on the host at each launch). */
