@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <array>
 #include <cstdlib>
+#include <cctype>
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -29,6 +30,7 @@
 #include <vector>
 
 #include "../axtb_b200/csrc/params/gfn2_tables.h"
+#include "../axtb_b200/csrc/params/solvation_tables.h"
 
 using namespace gfn2tab;
 using std::vector;
@@ -1687,6 +1689,473 @@ double entropy_tblite(const vector<double>& occ, double kt) {
     return s * kt;
 }
 
+// ============================================================================ solvation
+// Implicit solvation (ALPB, GBSA) of crates/solvation/src as a charge-dependent SCF term
+// (crates/axtb/src/solvation.rs:40-110): setup lib.rs:389-497, geometry lib.rs:553-627 (Born
+// radii born.rs:103-157, surface sasa.rs:31-240, kernel kernel.rs:28-66, shape kernel.rs:163-196),
+// energy and potential lib.rs:636-690, gradient lib.rs:692-712 (kernel.rs:70-160, born.rs:160-216,
+// kernel.rs:198-238). axtb's and tblite's conventions use its corrected variant (CODATA 2022
+// radii and constants), the xtb 6.8.0 conventions xtb's (mctc-lib's bohr factor and xtb's
+// constants in the free-energy shift); both recompute r1 for every pair of the Born integral.
+const double HARTREE_TO_KCAL_PER_MOL = 4.3597447222060e-18 * 6.02214076e23 / 4184.0;  // units.rs:37
+const double IDEAL_GAS_MOL_VOLUME_EXACT = 6.02214076e23 * 1.380649e-23 * 298.15 / 1.0e5 * 1.0e3;  // lib.rs:128
+const double XTB680_AATOAU = 1.0 / 5.29177210904492434e-1;  // units.rs:88
+
+struct Solv {
+    int nat = 0;
+    bool alpb = false, lhb = false;
+    double keps = 0, alpbet = 0, c1 = 0, gshift = 0, lrcut = 0, srcut = 0, w = 0, ah0 = 0, ah1 = 0, ah3 = 0;
+    vector<double> vdwr, rho, svdw, vdwsa, t1, t2, wrp, gamsasa, hbmag;
+    // geometry
+    vector<double> brad, dbrad, sasa, hbw, dhbdw, B, dsdr;
+    double adet = 0.0;
+    vector<vector<int>> nb;                       // SASA neighbours of each atom, ascending
+    vector<vector<std::array<double, 3>>> nbg;   // d sasa_i / d R_j per neighbour
+    vector<std::array<double, 3>> selfg;          // d sasa_i / d R_i
+};
+
+// free-energy shift of a reference state (lib.rs:277-306): 0 gsolv, 1 bar1M, 2 reference
+double solv_state_shift(int state, double temp, double density, double mass, double kb, double vm) {
+    using namespace solvtab;
+    if (state == 0) return 0.0;
+    double s = std::log(vm * temp / AMBIENT_TEMPERATURE);
+    if (state == 2) s += std::log(density / REF_DENSITY * REF_MOLECULAR_MASS / mass);
+    return temp * kb * s;
+}
+
+// the parameter set of a solvent name (lib.rs:255-272: lower case, xtb's aliases, the model's table)
+const solvtab::SolventParam* solv_lookup(const char* name, bool alpb) {
+    using namespace solvtab;
+    std::string s(name ? name : "");
+    size_t a = s.find_first_not_of(" \t\n"), b = s.find_last_not_of(" \t\n");
+    s = a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+    for (char& c : s) c = (char)std::tolower((unsigned char)c);
+    for (const auto& al : ALIASES)
+        if (s == al.alias) {
+            s = al.name;
+            break;
+        }
+    if (alpb) {
+        for (const auto& t : ALPB_SOLVENTS)
+            if (s == t.name) return &PARAMS[t.param];
+    } else {
+        for (const auto& t : GBSA_SOLVENTS)
+            if (s == t.name) return &PARAMS[t.param];
+    }
+    return nullptr;
+}
+
+Solv solv_setup(const Mol& m, int model, const char* solvent, int state) {
+    using namespace solvtab;
+    Solv sv;
+    sv.nat = m.nat;
+    sv.alpb = model == 0;
+    for (int z : m.Z)
+        if (z > NELEM) throw Fail(1, "solvation: unsupported element");
+    const SolventParam* p = solv_lookup(solvent, sv.alpb);
+    if (!p) throw Fail(1, "solvation: unknown solvent");
+    bool xtb = g_conv.id == 1;
+    double aatoau = xtb ? XTB680_AATOAU : AATOAU;
+    const double temp = DEFAULT_TEMPERATURE;
+    sv.gshift = xtb ? p->gshift * (1.0 / AUTOKCAL) + solv_state_shift(state, temp, p->rhos, p->smass, KB, IDEAL_GAS_MOL_VOLUME)
+                    : p->gshift / HARTREE_TO_KCAL_PER_MOL +
+                          solv_state_shift(state, temp, p->rhos, p->smass, KB_HARTREE, IDEAL_GAS_MOL_VOLUME_EXACT);
+    double eps = p->epsv;
+    sv.c1 = p->c1;
+    double offset = p->soset * 0.1 * aatoau, probe = p->rprobe * aatoau;
+    bool any_hb = false;
+    for (double t : p->tmp) any_hb = any_hb || std::fabs(t) > 1.0e-3;
+    sv.alpbet = sv.alpb ? ALPB_ALPHA / eps : 0.0;
+    sv.keps = (1.0 / eps - 1.0) / (1.0 + sv.alpbet);
+    sv.lrcut = LRCUT_AA * aatoau;
+    double w = SMOOTH_W_AA * aatoau, w3 = w * (w * w);
+    sv.w = w;
+    sv.ah0 = 0.5;
+    sv.ah1 = 3.0 / (4.0 * w);
+    sv.ah3 = -1.0 / (4.0 * w3);
+    double maxsa = -INFINITY;
+    for (int z : m.Z) {
+        int iz = z - 1;
+        double rvdw = aatoau * VDW_RAD_D3_AA[iz];
+        sv.vdwr.push_back(rvdw);
+        sv.rho.push_back(rvdw * p->sx[iz]);
+        sv.svdw.push_back(rvdw - offset);
+        double rsa = rvdw + probe;
+        sv.vdwsa.push_back(rsa);
+        maxsa = std::max(maxsa, rsa);
+        sv.t1.push_back((rsa - w) * (rsa - w));
+        sv.t2.push_back((rsa + w) * (rsa + w));
+        double r = rsa + w;
+        double wr = (0.25 / w + 3.0 * sv.ah3 * (0.2 * r * r - 0.5 * r * rsa + rsa * rsa / 3.0)) * r * r * r;
+        r = rsa - w;
+        wr -= (0.25 / w + 3.0 * sv.ah3 * (0.2 * r * r - 0.5 * r * rsa + rsa * rsa / 3.0)) * r * r * r;
+        sv.wrp.push_back(wr);
+        sv.gamsasa.push_back(p->gamscale[iz] * (4.0 * PI) * SURFACE_TENSION);
+        sv.hbmag.push_back(any_hb ? -(p->tmp[iz] * p->tmp[iz]) * (1.0 / AUTOKCAL) : 0.0);
+        if (sv.hbmag.back() < 0.0) sv.lhb = true;
+    }
+    sv.srcut = 2.0 * (w + maxsa) + SRCUT_AA * aatoau;
+    return sv;
+}
+
+// one pair of the Born integral (born.rs:13-96): the contributions to psi_i and psi_j and their
+// derivatives over r; r1 = 1/r for every pair
+struct PsiC {
+    bool on = false;
+    double g = 0.0, dg = 0.0;
+};
+inline PsiC psi_nonoverlap(double r, double rho, double r1) {
+    double ap = r + rho, am = r - rho, ab = ap * am, rhab = rho / ab;
+    double lnab = 0.5 * std::log(am / ap) * r1;
+    return {true, rhab + lnab, -2.0 * rhab / ab + (rhab - lnab) * r1 * r1};
+}
+inline PsiC psi_overlap(double r, double rho, double rvdw) {
+    double r1 = 1.0 / r, r12 = 0.5 * r1, r24 = r12 * r12;
+    double ap = r + rho, am = r - rho, rh1 = 1.0 / rvdw, rhr1 = 1.0 / ap, aprh1 = ap * rh1;
+    double lnab = std::log(aprh1);
+    double g = rh1 - rhr1 + r12 * (0.5 * am * (rhr1 - rh1 * aprh1) - lnab);
+    double dg = rhr1 * rhr1 * (1.0 - 0.25 * am * r1 * (1.0 + aprh1 * aprh1)) + rho * r24 * (rhr1 - rh1 * aprh1) +
+                r12 * (r1 * lnab - rhr1);
+    return {true, g, dg * r1};
+}
+void psi_pair(double r, double rhoi, double rhoj, double rvi, double rvj, PsiC& ci, PsiC& cj) {
+    double r1 = 1.0 / r;
+    bool ovij = !(r >= rvi + rhoj), ovji = !(r >= rhoi + rvj);
+    ci = PsiC{};
+    cj = PsiC{};
+    if (!ovij && !ovji) {
+        ci = psi_nonoverlap(r, rhoj, r1);
+        cj = std::fabs(rhoi - rhoj) < 1.0e-8 ? ci : psi_nonoverlap(r, rhoi, r1);
+    } else if (!ovij && ovji) {
+        ci = psi_nonoverlap(r, rhoj, r1);
+        if (r + rhoi > rvj) cj = psi_overlap(r, rhoi, rvj);
+    } else if (ovij && !ovji) {
+        if (r + rhoj > rvi) ci = psi_overlap(r, rhoj, rvi);
+        cj = psi_nonoverlap(r, rhoi, r1);
+    } else {
+        if (r + rhoj > rvi) ci = psi_overlap(r, rhoj, rvi);
+        if (r + rhoi > rvj) cj = psi_overlap(r, rhoi, rvj);
+    }
+}
+
+double adet_inertia(const Mol& m, const vector<double>& rad, double in[3][3], double center[3]) {
+    const double TOF = 2.0 / 5.0;
+    double tot = 0.0;
+    center[0] = center[1] = center[2] = 0.0;
+    for (int i = 0; i < m.nat; i++) {
+        double r3 = rad[i] * rad[i] * rad[i];
+        tot += r3;
+        for (int k = 0; k < 3; k++) center[k] += m.R(i)[k] * r3;
+    }
+    for (int k = 0; k < 3; k++) center[k] /= tot;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) in[a][b] = 0.0;
+    for (int i = 0; i < m.nat; i++) {
+        double r2 = rad[i] * rad[i], r3 = r2 * rad[i];
+        double v[3] = {m.R(i)[0] - center[0], m.R(i)[1] - center[1], m.R(i)[2] - center[2]};
+        double d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        double diag = r3 * (d2 + TOF * r2);
+        for (int k = 0; k < 3; k++) in[k][k] += diag;
+        for (int c = 0; c < 3; c++)
+            for (int r = 0; r < 3; r++) in[r][c] -= r3 * v[c] * v[r];
+    }
+    return tot;
+}
+double det3(const double a[3][3]) {
+    return a[0][0] * a[1][1] * a[2][2] - a[0][0] * a[1][2] * a[2][1] - a[0][1] * a[1][0] * a[2][2] +
+           a[0][1] * a[1][2] * a[2][0] + a[0][2] * a[1][0] * a[2][1] - a[0][2] * a[1][1] * a[2][0];
+}
+
+void solv_geometry(Solv& sv, const Mol& m) {
+    using namespace solvtab;
+    int n = m.nat;
+    auto dist = [&](int i, int j, double v[3]) {
+        for (int k = 0; k < 3; k++) v[k] = m.R(i)[k] - m.R(j)[k];
+        return v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    };
+    // Born radii (GBOBC-II)
+    sv.brad.assign(n, 0.0);
+    sv.dbrad.assign(n, 0.0);
+    vector<double>& psi = sv.brad;
+    double lr2 = sv.lrcut * sv.lrcut;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++) {
+            double v[3], d2 = dist(i, j, v);
+            if (!(d2 < lr2)) continue;
+            PsiC ci, cj;
+            psi_pair(std::sqrt(d2), sv.rho[i], sv.rho[j], sv.vdwr[i], sv.vdwr[j], ci, cj);
+            if (ci.on) psi[i] += ci.g;
+            if (cj.on) psi[j] += cj.g;
+        }
+    for (int i = 0; i < n; i++) {
+        double br = psi[i], s1 = 1.0 / sv.svdw[i], v1 = 1.0 / sv.vdwr[i], s2 = 0.5 * sv.svdw[i];
+        br *= s2;
+        double arg2 = br * (OBC_GAMMA * br - OBC_BETA);
+        double arg = br * (OBC_ALPHA + arg2);
+        arg2 = 2.0 * arg2 + OBC_ALPHA + OBC_GAMMA * br * br;
+        double th = std::tanh(arg), ch = std::cosh(arg);
+        double out = 1.0 / (s1 - v1 * th) * sv.c1;
+        double dpsi = ch * (s1 - v1 * th);
+        dpsi = s2 * v1 * arg2 / (dpsi * dpsi) * sv.c1;
+        psi[i] = out;
+        sv.dbrad[i] = dpsi;
+    }
+    // surface areas and their derivatives
+    sv.nb.assign(n, {});
+    double sr2 = sv.srcut * sv.srcut;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++) {
+            double v[3], d2 = dist(i, j, v);
+            double rmax = sv.vdwsa[i] + sv.vdwsa[j] + sv.w + 1.0e-6;
+            if (d2 < sr2 && d2 < rmax * rmax) {
+                sv.nb[i].push_back(j);
+                sv.nb[j].push_back(i);
+            }
+        }
+    for (auto& l : sv.nb) std::sort(l.begin(), l.end());
+    sv.sasa.assign(n, 0.0);
+    sv.selfg.assign(n, {0.0, 0.0, 0.0});
+    sv.nbg.assign(n, {});
+    for (int i = 0; i < n; i++) {
+        const vector<int>& nl = sv.nb[i];
+        int nno = (int)nl.size();
+        vector<std::array<double, 3>> grads(nno, {0.0, 0.0, 0.0});
+        vector<double> tj2(nno);
+        vector<int> gi(nno);
+        vector<std::array<double, 3>> gs(nno);
+        std::array<double, 3> gself = {0.0, 0.0, 0.0};
+        double sasai = 0.0, rsa = sv.vdwsa[i];
+        for (int ip = 0; ip < 230; ip++) {
+            const double* g = LEBEDEV_230[ip];
+            double xp[3] = {m.R(i)[0] + rsa * g[0], m.R(i)[1] + rsa * g[1], m.R(i)[2] + rsa * g[2]};
+            bool buried = false;
+            for (int s = 0; s < nno; s++) {
+                int j = nl[s];
+                double dx = xp[0] - m.R(j)[0], dy = xp[1] - m.R(j)[1], dz = xp[2] - m.R(j)[2];
+                tj2[s] = dx * dx + dy * dy + dz * dz;
+                buried = buried || tj2[s] <= sv.t1[j];
+            }
+            if (buried) continue;
+            int nni = 0;
+            double sasap = 1.0;
+            for (int s = 0; s < nno; s++) {
+                int j = nl[s];
+                if (!(tj2[s] < sv.t2[j])) continue;
+                double tj[3] = {xp[0] - m.R(j)[0], xp[1] - m.R(j)[1], xp[2] - m.R(j)[2]};
+                double sq = std::sqrt(tj2[s]), uj = sq - sv.vdwsa[j], ah3uj2 = sv.ah3 * uj * uj;
+                double ds = sv.ah1 + 3.0 * ah3uj2;
+                double sij = sv.ah0 + (sv.ah1 + ah3uj2) * uj;
+                if (1.0 < sij) sij = 1.0;
+                if (0.0 > sij) sij = 0.0;
+                if (sij < DBL_MIN) {
+                    sasap = 0.0;
+                    break;
+                }
+                sasap *= sij;
+                ds /= sij * sq;
+                gi[nni] = s;
+                gs[nni] = {ds * tj[0], ds * tj[1], ds * tj[2]};
+                nni++;
+            }
+            if (sasap > TOLSESP) {
+                double wsa = g[3] * sv.wrp[i] * sasap;
+                sasai += wsa;
+                for (int q = 0; q < nni; q++)
+                    for (int k = 0; k < 3; k++) {
+                        double d = wsa * gs[q][k];
+                        gself[k] += d;
+                        grads[gi[q]][k] -= d;
+                    }
+            }
+        }
+        sv.sasa[i] = sasai;
+        sv.selfg[i] = gself;
+        sv.nbg[i] = grads;
+    }
+    sv.dsdr.assign(3 * n, 0.0);
+    for (int i = 0; i < n; i++) {
+        double c = sv.gamsasa[i];
+        if (c == 0.0) continue;
+        for (int k = 0; k < 3; k++) sv.dsdr[3 * i + k] += sv.selfg[i][k] * c;
+        for (size_t s = 0; s < sv.nb[i].size(); s++)
+            for (int k = 0; k < 3; k++) sv.dsdr[3 * sv.nb[i][s] + k] += sv.nbg[i][s][k] * c;
+    }
+    sv.hbw.assign(n, 0.0);
+    sv.dhbdw.assign(n, 0.0);
+    if (sv.lhb)
+        for (int i = 0; i < n; i++) {
+            double smaxd = 1.0 / (sv.vdwsa[i] * sv.vdwsa[i]);
+            sv.hbw[i] = sv.hbmag[i] * (sv.sasa[i] * smaxd);
+            sv.dhbdw[i] = sv.hbmag[i] * smaxd;
+        }
+    sv.adet = 0.0;
+    if (sv.alpbet > 0.0) {
+        double in[3][3], c[3];
+        double tot = adet_inertia(m, sv.vdwr, in, c);
+        sv.adet = std::sqrt(std::pow(det3(in), 1.0 / 3.0) / ((2.0 / 5.0) * tot));
+    }
+    // Born matrix: P16 (ALPB) or Still (GBSA) kernel, H-bond diagonal, ALPB shape term
+    sv.B.assign((size_t)n * n, 0.0);
+    const double zo16 = ZETA_P16 / 16.0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < i; j++) {
+            double v[3], r = std::sqrt(dist(i, j, v)), val;
+            if (sv.alpb) {
+                double ab = std::sqrt(sv.brad[i] * sv.brad[j]);
+                double arg = ab / (ab + zo16 * r);
+                arg *= arg;
+                arg *= arg;
+                arg *= arg;
+                arg *= arg;
+                val = sv.keps * (1.0 / (r + ab * arg));
+            } else {
+                double r2 = r * r, aa = sv.brad[i] * sv.brad[j], dd = 0.25 * r2 / aa;
+                val = sv.keps * (1.0 / std::sqrt(r2 + aa * std::exp(-dd)));
+            }
+            sv.B[(size_t)i * n + j] = sv.B[(size_t)j * n + i] = val;
+        }
+    for (int i = 0; i < n; i++) sv.B[(size_t)i * n + i] = sv.keps * (1.0 / sv.brad[i]);
+    if (sv.lhb)
+        for (int i = 0; i < n; i++) sv.B[(size_t)i * n + i] += 2.0 * sv.hbw[i];
+    if (sv.alpbet > 0.0) {
+        double shift = sv.keps * sv.alpbet / sv.adet;
+        for (double& x : sv.B) x += shift;
+    }
+}
+
+// dot product with four interleaved partial sums (lib.rs:742-758)
+double dot4(const double* a, const double* b, int n) {
+    double acc[4] = {0, 0, 0, 0};
+    int n4 = n / 4 * 4;
+    for (int i = 0; i < n4; i += 4)
+        for (int k = 0; k < 4; k++) acc[k] += a[i + k] * b[i + k];
+    double s = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+    for (int i = n4; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+// fixed part: surface term and shift (lib.rs:636-652)
+double solv_fixed(const Solv& sv, vector<double>* g) {
+    double e = 0.0, shift = sv.gshift / sv.nat;
+    for (int i = 0; i < sv.nat; i++) e += sv.sasa[i] * sv.gamsasa[i] + shift;
+    if (g)
+        for (int k = 0; k < 3 * sv.nat; k++) (*g)[k] += sv.dsdr[k];
+    return e;
+}
+// charge-dependent energy 1/2 q^T B q (lib.rs:654-664) and potential B q (lib.rs:666-675)
+double solv_energy(const Solv& sv, const vector<double>& q) {
+    double e = 0.0;
+    for (int i = 0; i < sv.nat; i++) e += q[i] * (0.5 * dot4(&sv.B[(size_t)i * sv.nat], q.data(), sv.nat));
+    return e;
+}
+void solv_potential(const Solv& sv, const vector<double>& q, vector<double>& vat) {
+    for (int i = 0; i < sv.nat; i++) vat[i] += dot4(&sv.B[(size_t)i * sv.nat], q.data(), sv.nat);
+}
+
+// explicit gradient of 1/2 q^T B q at fixed charges (lib.rs:692-712)
+void solv_gradient(const Solv& sv, const Mol& m, const vector<double>& q, vector<double>& grad) {
+    int n = sv.nat;
+    vector<double> dedbr(n, 0.0);
+    const double zo16 = solvtab::ZETA_P16 / 16.0;
+    for (int i = 0; i < n; i++) {
+        double gi[3] = {0, 0, 0}, di = 0.0;
+        for (int j = 0; j < i; j++) {
+            double v[3] = {m.R(i)[0] - m.R(j)[0], m.R(i)[1] - m.R(j)[1], m.R(i)[2] - m.R(j)[2]};
+            double r = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]), qq = q[i] * q[j];
+            if (sv.alpb) {
+                double ab = std::sqrt(sv.brad[i] * sv.brad[j]);
+                double a1 = ab / (ab + zo16 * r), a16 = a1 * a1;
+                a16 *= a16;
+                a16 *= a16;
+                a16 *= a16;
+                double fgb = r + ab * a16, dfgb = 1.0 / fgb, dfgb2 = dfgb * dfgb;
+                double ap = (1.0 - solvtab::ZETA_P16 * a1 * a16) * dfgb2;
+                for (int k = 0; k < 3; k++) {
+                    double dg = ap * v[k] * sv.keps / r * qq;
+                    gi[k] -= dg;
+                    grad[3 * j + k] += dg;
+                }
+                double bp = -0.5 * (r * solvtab::ZETA_P16 / ab * a1 + 1.0) / ab * a16 * dfgb2;
+                di += sv.brad[j] * bp * sv.keps * qq;
+                dedbr[j] += sv.brad[i] * bp * sv.keps * qq;
+            } else {
+                double r2 = r * r, aa = sv.brad[i] * sv.brad[j], dd = 0.25 * r2 / aa, expd = std::exp(-dd);
+                double fgb2 = r2 + aa * expd, dfgb2 = 1.0 / fgb2, dfgb = std::sqrt(dfgb2);
+                double dfgb3 = dfgb2 * dfgb * sv.keps, ap = (1.0 - 0.25 * expd) * dfgb3;
+                for (int k = 0; k < 3; k++) {
+                    double dr = ap * v[k];
+                    gi[k] -= dr * qq;
+                    grad[3 * j + k] += dr * qq;
+                }
+                double bp = -0.5 * expd * (1.0 + dd) * dfgb3;
+                di += sv.brad[j] * bp * qq;
+                dedbr[j] += sv.brad[i] * bp * qq;
+            }
+        }
+        for (int k = 0; k < 3; k++) grad[3 * i + k] += gi[k];
+        dedbr[i] += di;
+    }
+    for (int i = 0; i < n; i++) {
+        double bp = 1.0 / sv.brad[i], qq = q[i] * bp;
+        dedbr[i] += -0.5 * sv.keps * qq * bp * q[i];
+    }
+    // Born radii chain: sum_i (dE/dbrad_i dbrad_i/dpsi_i) dpsi_i/dR
+    for (int i = 0; i < n; i++) dedbr[i] *= sv.dbrad[i];
+    double lr2 = sv.lrcut * sv.lrcut;
+    for (int i = 0; i < n; i++) {
+        double gi[3] = {0, 0, 0};
+        for (int j = 0; j < i; j++) {
+            double v[3] = {m.R(i)[0] - m.R(j)[0], m.R(i)[1] - m.R(j)[1], m.R(i)[2] - m.R(j)[2]};
+            double d2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            if (!(d2 < lr2)) continue;
+            PsiC ci, cj;
+            psi_pair(std::sqrt(d2), sv.rho[i], sv.rho[j], sv.vdwr[i], sv.vdwr[j], ci, cj);
+            double s = 0.0;
+            if (ci.on) s += dedbr[i] * ci.dg;
+            if (cj.on) s += dedbr[j] * cj.dg;
+            if (s != 0.0)
+                for (int k = 0; k < 3; k++) {
+                    gi[k] += s * v[k];
+                    grad[3 * j + k] -= s * v[k];
+                }
+        }
+        for (int k = 0; k < 3; k++) grad[3 * i + k] += gi[k];
+    }
+    // H-bond term through the surface
+    if (sv.lhb)
+        for (int i = 0; i < n; i++) {
+            double c = sv.dhbdw[i] * q[i] * q[i];
+            if (c == 0.0) continue;
+            for (int k = 0; k < 3; k++) grad[3 * i + k] += sv.selfg[i][k] * c;
+            for (size_t s = 0; s < sv.nb[i].size(); s++)
+                for (int k = 0; k < 3; k++) grad[3 * sv.nb[i][s] + k] += sv.nbg[i][s][k] * c;
+        }
+    // ALPB shape term (kernel.rs:198-238)
+    if (sv.alpbet > 0.0) {
+        double qt = 0.0;
+        for (double x : q) qt += x;
+        double in[3][3], c[3];
+        double tot = adet_inertia(m, sv.vdwr, in, c);
+        double adet = std::sqrt(std::pow(det3(in), 1.0 / 3.0) / ((2.0 / 5.0) * tot));
+        double t2 = tot * tot, a2 = adet * adet;
+        double fa = 250.0 / (48.0 * (t2 * tot) * ((a2 * a2) * adet));
+        double fb = -0.5 * sv.keps * sv.alpbet * (qt * qt) / a2;
+        auto f = [&](double x) { return x * fa * fb; };
+        double xy = in[0][1] * in[2][2] - in[0][2] * in[1][2];
+        double xz = in[0][2] * in[1][1] - in[0][1] * in[2][1];
+        double yz = in[0][0] * in[1][2] - in[0][1] * in[0][2];
+        double xx = in[0][0] * (in[1][1] + in[2][2]) - in[0][1] * in[0][1] - in[0][2] * in[0][2];
+        double yy = in[1][1] * (in[0][0] + in[2][2]) - in[0][1] * in[0][1] - in[1][2] * in[1][2];
+        double zz = in[2][2] * (in[0][0] + in[1][1]) - in[0][2] * in[0][2] - in[1][2] * in[1][2];
+        double d[3][3] = {{f(xx), f(xy), f(xz)}, {f(xy), f(yy), f(yz)}, {f(xz), f(yz), f(zz)}};
+        for (int i = 0; i < n; i++) {
+            double r3 = sv.vdwr[i] * sv.vdwr[i] * sv.vdwr[i];
+            double v[3] = {m.R(i)[0] - c[0], m.R(i)[1] - c[1], m.R(i)[2] - c[2]};
+            for (int k = 0; k < 3; k++) grad[3 * i + k] += r3 * (d[k][0] * v[0] + d[k][1] * v[1] + d[k][2] * v[2]);
+        }
+    }
+}
+
 // ============================================================================ Broyden
 // modified Broyden mixing of crates/axtb/src/scf/mixing.rs:185-338 (memory = max_iter) with
 // Gauss elimination crates/base/src/linalg/lu.rs:81-112
@@ -1982,6 +2451,16 @@ int run(OracleRun* R) {
     vector<double> grad(3 * nat, 0.0), dedcn(nat, 0.0);
     double e_rep = repulsion(md, wantg ? &grad : nullptr);
     double e_atm = d4_atm(d4, m, wantg ? &grad : nullptr);
+    // implicit solvation: geometry part, surface energy and shift (crates/axtb/src/solvation.rs:66-75)
+    bool solv = R->solv_model >= 0;
+    Solv sv;
+    double e_solv_fixed = 0.0;
+    if (solv) {
+        if (R->solv_model > 1 || R->solv_state < 0 || R->solv_state > 2) throw Fail(1, "solvation: unknown model or state");
+        sv = solv_setup(m, R->solv_model, R->solvent, R->solv_state);
+        solv_geometry(sv, m);
+        e_solv_fixed = solv_fixed(sv, wantg ? &grad : nullptr);
+    }
     Ints I = build_ints(md, se);
     GenEig eig;
     eig.init(I.S, nao, R->eig_backend == 1);
@@ -2052,6 +2531,7 @@ int run(OracleRun* R) {
             for (int a = 0; a < nsh; a++) pot.vsh[a] += state.qsh[a] * state.qsh[a] * md.gam3[a];
             aes_potential(md, ac, state.qat, state.dp, state.qp, pot.vat, pot.vdp, pot.vqp);
             d4_energy(d4, state.qat, &pot.vat);
+            if (solv) solv_potential(sv, state.qat, pot.vat);
             // Fock (crates/axtb/src/scf/fock.rs:22-104)
             vector<double> B((size_t)nao * nao);
             for (int nu = 0; nu < nao; nu++) {
@@ -2137,7 +2617,8 @@ int run(OracleRun* R) {
             double edisp = d4_energy(d4, out.qat, nullptr);
             double band = 0.0;
             for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
-            double energy = e2 + e3 + eaes + edisp + ts + band;
+            double esolv = solv ? solv_energy(sv, out.qat) : 0.0;
+            double energy = e2 + e3 + eaes + edisp + ts + band + esolv;
             if (!std::isfinite(energy)) throw Fail(4, "non-finite energy");
             double res = 0.0;
             for (double x : mix.dq) res += x * x;
@@ -2165,7 +2646,7 @@ int run(OracleRun* R) {
     R->converged = converged;
     terms[0] = e_rep;
     terms[1] += e_atm;
-    double energy = e_rep + e_atm + terms[2];
+    double energy = e_rep + e_atm + terms[2] + e_solv_fixed;
     if (R->energy) *R->energy = energy;
     if (R->terms) std::memcpy(R->terms, terms, sizeof terms);
     if (R->qat) std::copy(out.qat.begin(), out.qat.end(), R->qat);
@@ -2216,6 +2697,7 @@ int run(OracleRun* R) {
         es2_grad(md, out.qsh, grad);
         aes_grad(md, ac, out.qat, out.dp, out.qp, grad, dedcn);
         d4_grad(d4, m, out.qat, grad);
+        if (solv) solv_gradient(sv, m, out.qat, grad);
         // H0/S/D/Q derivative contraction (crates/axtb/src/hamiltonian.rs:101-223)
         vector<double> vao(nao);
         for (int mu = 0; mu < nao; mu++) vao[mu] = pot.vsh[b.ao2sh[mu]] + pot.vat[b.ao2at[mu]];

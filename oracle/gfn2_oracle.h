@@ -30,6 +30,9 @@ typedef struct {
     int mixer;               /* -1: the conventions' mixer; 0: auto (Broyden, then DIIS from the
                                 start guess), 1: Broyden, 2: DIIS */
     int conventions;         /* 0: axtb (default), 1: the xtb 6.8.0 program's, 2: tblite 0.8.0's */
+    int solv_model;          /* implicit solvation: -1 none, 0 ALPB, 1 GBSA */
+    const char* solvent;     /* solvent name (xtb's names and aliases) */
+    int solv_state;          /* reference state: 0 gsolv, 1 bar1M, 2 reference */
     /* outputs (caller-allocated; any may be NULL) */
     double* energy;
     double* gradient;        /* nat*3 */

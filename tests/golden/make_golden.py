@@ -13,8 +13,12 @@ structures, multielement, charges, spin, etemp_acc, open_shell_metals, threads) 
 
 with numbers, positions (bohr), charge, uhf, accuracy, etemp, max_iter and the recorded axtb
 results, plus axtb's energies and iterations in its xtb (6.8.0) and tblite (0.8.0) conventions
-(``programs["axtb[xtb]"]``, ``programs["axtb[tblite]"]``). Run once in a checkout that has the
-axtb sources::
+(``programs["axtb[xtb]"]``, ``programs["axtb[tblite]"]``); and, in
+
+    tests/golden/solvation.json
+
+the cases of the solvation category (ALPB or GBSA, solvent, reference state) with axtb's recorded
+energies. Run once in a checkout that has the axtb sources::
 
     python tests/golden/make_golden.py [path-to-axtb-checkout]
 """
@@ -26,6 +30,7 @@ from pathlib import Path
 
 REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
 OUT = Path(__file__).with_name("reference_matrix.json")
+SOLV = Path(__file__).with_name("solvation.json")
 KEEP = {"elements", "structures", "multielement", "charges", "spin", "etemp_acc", "open_shell_metals", "threads"}
 
 
@@ -69,6 +74,25 @@ def main() -> None:
     OUT.write_text(json.dumps({"source": "axtb tests/reference_matrix/results.json (programs.axtb)",
                                "cases": out}, indent=0))
     print(f"wrote {len(out)} cases to {OUT}")
+    # implicit solvation (category solvation): ALPB or GBSA, solvent, reference state (gsolv when
+    # the case names none), axtb's recorded energy in its default conventions
+    solv = []
+    for c in C.CATEGORIES["solvation"]():
+        r = results.get(c["id"])
+        ax = (r or {}).get("programs", {}).get("axtb")
+        if not ax or not ax.get("ok") or "energy" not in ax:
+            continue
+        model = "alpb" if "alpb" in c else "gbsa"
+        solv.append({
+            "id": c["id"], "numbers": c["numbers"], "positions": c["positions"], "charge": c["charge"],
+            "uhf": c["uhf"], "accuracy": c.get("accuracy", 1.0), "etemp": c.get("etemp", 300.0),
+            "max_iter": c.get("max_iter", 250), "model": model, "solvent": c[model],
+            "state": c.get("solvation_state") or "gsolv", "energy": ax["energy"],
+            "iterations": ax.get("iterations"),
+        })
+    SOLV.write_text(json.dumps({"source": "axtb tests/reference_matrix/results.json (programs.axtb, "
+                                          "category solvation)", "cases": solv}, indent=0))
+    print(f"wrote {len(solv)} cases to {SOLV}")
 
 
 if __name__ == "__main__":
