@@ -27,7 +27,8 @@ DBG = {"cn": 0, "overlap": 1, "h0": 2, "dipole": 3, "quadrupole": 4, "density": 
 class AxtbOptions(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("etemp", C.c_double), ("max_iter", C.c_int32), ("damping", C.c_double),
                 ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("mixer", C.c_int32),
-                ("conventions", C.c_int32)]
+                ("conventions", C.c_int32), ("solvation", C.c_int32), ("solvent", C.c_char_p),
+                ("solvation_state", C.c_int32)]
 
 
 class AxtbResult(C.Structure):

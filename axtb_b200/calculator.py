@@ -105,12 +105,29 @@ def _conventions(name: str) -> int:
         raise AxtbError(1, f"unknown conventions {name!r} (axtb, xtb or tblite)") from None
 
 
+# implicit solvation: (model "alpb" | "gbsa", solvent, reference state "gsolv" | "bar1M" | "reference")
+SOLVATION_MODELS = {"alpb": 0, "gbsa": 1}
+SOLVATION_STATES = {"gsolv": 0, "bar1m": 1, "reference": 2}
+
+
+def _solvation(spec):
+    if spec is None:
+        return -1, None, 0
+    model, solvent, *state = spec
+    try:
+        return SOLVATION_MODELS[model.lower()], solvent.encode(), SOLVATION_STATES[(state[0] if state else "gsolv").lower()]
+    except KeyError:
+        raise AxtbError(1, f"unknown solvation model or state in {spec!r}") from None
+
+
 def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0,
-             mixer=None, conventions="axtb"):
+             mixer=None, conventions="axtb", solvation=None):
+    model, solvent, state = _solvation(solvation)
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
                                 damping=float(damping), guess=0 if guess == "eeq" else 1,
                                 precision={"fp64": 0, "split": 1}[precision], device=int(device),
-                                mixer=_mixer(mixer), conventions=_conventions(conventions))
+                                mixer=_mixer(mixer), conventions=_conventions(conventions), solvation=model,
+                                solvent=solvent, solvation_state=state)
 
 
 class Calculator:

@@ -26,6 +26,7 @@
 #include "k_geometry.cuh"
 #include "k_integrals.cuh"
 #include "k_scf.cuh"
+#include "k_solvation.cuh"
 #include "params/gfn2_tables.h"
 #include "team_kernel.cuh"
 
@@ -235,7 +236,33 @@ struct Opt {
     int max_iter = 250, guess = 0, precision = 0, device = 0;
     int mixer = -1;  // -1 the conventions' mixer, 0 auto (Broyden, then DIIS from the start), 1 Broyden, 2 DIIS
     int conventions = 0;  // 0 axtb, 1 xtb (6.8.0), 2 tblite (0.8.0)
+    int solv = -1;        // implicit solvation: -1 none, 0 ALPB, 1 GBSA
+    std::string solvent;  // its solvent (xtb's names and aliases)
+    int solv_state = 0;   // reference state: 0 gsolv, 1 bar1M, 2 reference
 };
+
+// ------------------------------------------------------------------ solvation parameters
+// the parameter set of a solvent name (crates/solvation/src/lib.rs:255-272: trimmed, lower case,
+// xtb's aliases, the model's table); nullptr when the model has none
+const solvtab::SolventParam* solvent_param(const std::string& name, bool alpb) {
+    using namespace solvtab;
+    size_t a = name.find_first_not_of(" \t\n"), b = name.find_last_not_of(" \t\n");
+    std::string s = a == std::string::npos ? std::string() : name.substr(a, b - a + 1);
+    for (char& c : s) c = (char)std::tolower((unsigned char)c);
+    for (const auto& al : ALIASES)
+        if (s == al.alias) {
+            s = al.name;
+            break;
+        }
+    if (alpb) {
+        for (const auto& t : ALPB_SOLVENTS)
+            if (s == t.name) return &PARAMS[t.param];
+    } else {
+        for (const auto& t : GBSA_SOLVENTS)
+            if (s == t.name) return &PARAMS[t.param];
+    }
+    return nullptr;
+}
 
 void check_options(const Opt& o) {
     if (!(o.acc > 0.0 && std::isfinite(o.acc))) throw Fail(AXTB_ERR_INPUT, "SCF accuracy must be a positive number");
@@ -245,6 +272,11 @@ void check_options(const Opt& o) {
     if (o.precision != 0 && o.precision != 1) throw Fail(AXTB_ERR_INPUT, "precision must be 0 (FP64) or 1 (split)");
     if (o.mixer < -1 || o.mixer > 2) throw Fail(AXTB_ERR_INPUT, "unknown SCF mixer (0 auto, 1 Broyden, 2 DIIS)");
     if (o.conventions < 0 || o.conventions > 2) throw Fail(AXTB_ERR_INPUT, "unknown conventions (0 axtb, 1 xtb, 2 tblite)");
+    if (o.solv < -1 || o.solv > 1) throw Fail(AXTB_ERR_INPUT, "unknown solvation model (-1 none, 0 ALPB, 1 GBSA)");
+    if (o.solv >= 0 && (o.solv_state < 0 || o.solv_state > 2))
+        throw Fail(AXTB_ERR_INPUT, "unknown solvation reference state (0 gsolv, 1 bar1M, 2 reference)");
+    if (o.solv >= 0 && !solvent_param(o.solvent, o.solv == 0))
+        throw Fail(AXTB_ERR_INPUT, "solvation: unknown solvent '" + o.solvent + "' for this model");
 }
 
 // ------------------------------------------------------------------ device arena
@@ -612,6 +644,11 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addD((size_t)nwk);
     addL(nmol * 5);
     addD((size_t)nsqT * 2);
+    if (o.solv >= 0) {  // solvation: 9 per-atom parameter arrays, 7 per-atom state arrays, lists
+        addD((size_t)natT * 9 + nmol);
+        addD((size_t)natT * 9 + nmol);
+        addI((size_t)natT * axg::SOLV_MAXNB + natT);
+    }
     bytes += 1 << 20;
     CK(cudaMalloc(&dmem, bytes));
     Arena ar{(char*)dmem, bytes, 0};
@@ -731,6 +768,76 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         }
         b.m_paircut2 = upD(pc);
     }
+    // implicit solvation (crates/solvation/src/lib.rs:394-497 paramToModel and initBorn): axtb's and
+    // tblite's conventions use the corrected variant (CODATA 2022 radii and constants), the xtb
+    // 6.8.0 conventions xtb's (mctc-lib's bohr factor, xtb's constants in the shift)
+    b.solv = o.solv >= 0 ? 1 : 0;
+    if (b.solv) {
+        using namespace solvtab;
+        const SolventParam* p = solvent_param(o.solvent, o.solv == 0);
+        bool xtbv = o.conventions == 1;
+        double aatoau = xtbv ? 1.0 / 5.29177210904492434e-1 : AATOAU;
+        const double temp = DEFAULT_TEMPERATURE;
+        auto shift = [&](double kb, double vm) {
+            if (o.solv_state == 0) return 0.0;
+            double s = std::log(vm * temp / AMBIENT_TEMPERATURE);
+            if (o.solv_state == 2) s += std::log(p->rhos / REF_DENSITY * REF_MOLECULAR_MASS / p->smass);
+            return temp * kb * s;
+        };
+        const double hartree_kcal = 4.3597447222060e-18 * 6.02214076e23 / 4184.0;
+        const double vm_exact = 6.02214076e23 * 1.380649e-23 * 298.15 / 1.0e5 * 1.0e3;
+        b.sv_gshift = xtbv ? p->gshift * (1.0 / AUTOKCAL) + shift(KB, IDEAL_GAS_MOL_VOLUME)
+                           : p->gshift / hartree_kcal + shift(KB_HARTREE, vm_exact);
+        double eps = p->epsv, offset = p->soset * 0.1 * aatoau, probe = p->rprobe * aatoau;
+        bool any_hb = false;
+        for (double t : p->tmp) any_hb = any_hb || std::fabs(t) > 1.0e-3;
+        b.sv_alpb = o.solv == 0 ? 1 : 0;
+        b.sv_alpbet = b.sv_alpb ? ALPB_ALPHA / eps : 0.0;
+        b.sv_keps = (1.0 / eps - 1.0) / (1.0 + b.sv_alpbet);
+        b.sv_c1 = p->c1;
+        b.sv_lrcut = LRCUT_AA * aatoau;
+        double w = SMOOTH_W_AA * aatoau, w3 = w * (w * w);
+        b.sv_w = w;
+        b.sv_ah0 = 0.5;
+        b.sv_ah1 = 3.0 / (4.0 * w);
+        b.sv_ah3 = -1.0 / (4.0 * w3);
+        vector<double> vdwr(natT), rho(natT), svdw(natT), vdwsa(natT), t1(natT), t2(natT), wrp(natT), gam(natT),
+            hbmag(natT), srcut(nmol);
+        for (int m = 0; m < nmol; m++) {
+            double maxsa = -INFINITY;
+            for (int i = 0; i < mols[m].nat; i++) {
+                int a = m_at0[m] + i, iz = mols[m].Z[i] - 1;
+                if (iz + 1 > NELEM) throw Fail(AXTB_ERR_INPUT, "solvation: unsupported element");
+                double rvdw = aatoau * VDW_RAD_D3_AA[iz], rsa = rvdw + probe;
+                vdwr[a] = rvdw;
+                rho[a] = rvdw * p->sx[iz];
+                svdw[a] = rvdw - offset;
+                vdwsa[a] = rsa;
+                maxsa = std::max(maxsa, rsa);
+                t1[a] = (rsa - w) * (rsa - w);
+                t2[a] = (rsa + w) * (rsa + w);
+                double r = rsa + w;
+                double wr = (0.25 / w + 3.0 * b.sv_ah3 * (0.2 * r * r - 0.5 * r * rsa + rsa * rsa / 3.0)) * r * r * r;
+                r = rsa - w;
+                wr -= (0.25 / w + 3.0 * b.sv_ah3 * (0.2 * r * r - 0.5 * r * rsa + rsa * rsa / 3.0)) * r * r * r;
+                wrp[a] = wr;
+                gam[a] = p->gamscale[iz] * (4.0 * PI_) * SURFACE_TENSION;
+                hbmag[a] = any_hb ? -(p->tmp[iz] * p->tmp[iz]) * (1.0 / AUTOKCAL) : 0.0;
+            }
+            srcut[m] = 2.0 * (w + maxsa) + SRCUT_AA * aatoau;
+        }
+        b.sv_vdwr = upD(vdwr);
+        b.sv_rho = upD(rho);
+        b.sv_svdw = upD(svdw);
+        b.sv_vdwsa = upD(vdwsa);
+        b.sv_t1 = upD(t1);
+        b.sv_t2 = upD(t2);
+        b.sv_wrp = upD(wrp);
+        b.sv_gam = upD(gam);
+        b.sv_hbmag = upD(hbmag);
+        b.sv_srcut = upD(srcut);
+        CK(cudaMemcpyToSymbolAsync(axg::c_lebedev, LEBEDEV_230, sizeof(LEBEDEV_230), 0, cudaMemcpyHostToDevice, st));
+    }
     b.damping = o.damping;
     b.econv = 1e-6 * o.acc;
     b.pconv = 2e-5 * o.acc;
@@ -816,6 +923,18 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.e_atom = ar.take<double>(natT);
     s.e_terms = ar.take<double>(natT * 5);
     s.mol_cyc = ar.take<double>(nmol);
+    if (o.solv >= 0) {
+        s.sv_brad = ar.take<double>(natT);
+        s.sv_dbrad = ar.take<double>(natT);
+        s.sv_sasa = ar.take<double>(natT);
+        s.sv_hbw = ar.take<double>(natT);
+        s.sv_dhbdw = ar.take<double>(natT);
+        s.sv_selfg = ar.take<double>((size_t)natT * 3);
+        s.sv_dedbr = ar.take<double>(natT);
+        s.sv_adet = ar.take<double>(nmol);
+        s.sv_nb = ar.take<int>((size_t)natT * axg::SOLV_MAXNB);
+        s.sv_nbn = ar.take<int>(natT);
+    }
     s.red = ar.take<double>((size_t)axg::team_red_doubles(grid));  // grid-team partials
     s.eeq_A = ar.take<double>((size_t)nsqT * 3);
     // team plan
@@ -1099,6 +1218,13 @@ void AxtbBatch::run(bool want_grad, bool warm) {
     LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm));
     // integrals
     LAUNCH("integrals", 0, mat_bytes(all, 11.0), k_integrals<<<blocks_for(npdT, 128), 128, 0, st>>>(B, S, d_pd0, npdT));
+    if (B.solv) {  // solvation: Born radii, SASA neighbours and surfaces, ALPB shape descriptor
+        unsigned wb = blocks_for((long long)natT * 32, T);
+        LAUNCH("solv_born", 0, 0, k_solv_born<<<wb, T, 0, st>>>(B, S));
+        LAUNCH("solv_neighbours", 0, 0, k_solv_neighbours<<<wb, T, 0, st>>>(B, S));
+        LAUNCH("solv_sasa", 0, 0, k_solv_sasa<<<wb, T, 0, st>>>(B, S));
+        LAUNCH("solv_adet", 0, 0, k_solv_adet<<<nmol, 32, 0, st>>>(B, S));
+    }
     // overlap factorisation and EEQ start
     void* args[] = {&B, &S, &P, nullptr};
     int ph = PH_OVERLAP;
@@ -1127,6 +1253,8 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         for (int it = 1; it <= opt.max_iter; it++) {
             LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_in, 0));
             LAUNCH("potentials", 0, 0, k_potentials<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+            if (B.solv)
+                LAUNCH("solv_potential", 0, 0, k_solv_potential<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
             LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
             ph = PH_EIGEN;
             LAUNCH("team_eigen", eig_flops(act), 0,
@@ -1136,6 +1264,8 @@ void AxtbBatch::run(bool want_grad, bool warm) {
             LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
             LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 2));
             LAUNCH("energy", 0, 0, k_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+            if (B.solv)
+                LAUNCH("solv_energy", 0, 0, k_solv_energy<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
             if (diis) LAUNCH("diis", 0, 0, k_diis<<<nmol, T, 0, st>>>(B, S));
             else LAUNCH("broyden", 0, 0, k_broyden<<<nmol, T, 0, st>>>(B, S, hist_cap));
             CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
@@ -1183,6 +1313,13 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         LAUNCH("h0_gather", 0, 0, k_h0_gather<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_pair0, S.pair_buf));
         LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, S.qat_out, 1));
         LAUNCH("grad_pairs", 0, 0, k_grad_pairs<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+        if (B.solv) {
+            unsigned wb = blocks_for((long long)natT * 32, T);
+            LAUNCH("solv_grad_kernel", 0, 0, k_solv_grad_kernel<<<wb, T, 0, st>>>(B, S));
+            LAUNCH("solv_grad_psi", 0, 0, k_solv_grad_psi<<<wb, T, 0, st>>>(B, S));
+            LAUNCH("solv_grad_surface", 0, 0, k_solv_grad_surface<<<wb, T, 0, st>>>(B, S));
+            LAUNCH("solv_grad_adet", 0, 0, k_solv_grad_adet<<<nmol, T, 0, st>>>(B, S));
+        }
         LAUNCH("cn_chain", 0, 0, k_cn_chain<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
     }
 #undef LAUNCH

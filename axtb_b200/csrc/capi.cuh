@@ -92,6 +92,9 @@ static Opt to_opt(const AxtbOptions* o) {
         r.device = o->device;
         r.mixer = o->mixer;
         r.conventions = o->conventions;
+        r.solv = o->solvation;
+        r.solvent = o->solvent ? o->solvent : "";
+        r.solv_state = o->solvation_state;
     }
     return r;
 }
@@ -137,6 +140,9 @@ void axtb_gpu_default_options(AxtbOptions* o) {
     o->device = 0;
     o->mixer = -1;
     o->conventions = 0;
+    o->solvation = -1;
+    o->solvent = nullptr;
+    o->solvation_state = 0;
 }
 
 int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao) {

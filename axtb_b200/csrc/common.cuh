@@ -26,6 +26,7 @@ enum : int {
     ST_HISTORY = 32,       // Broyden history capacity exhausted
     ST_TIMEOUT = 64,       // a bounded device wait gave up
     ST_FOCK = 128,         // non-finite Fock matrix
+    ST_SOLV = 256,         // an atom has more SASA neighbours than the solvation lists hold
 };
 
 struct Batch {
@@ -72,6 +73,12 @@ struct Batch {
     double cn_cut, rep_cut, d4_cn_cut, d2_cut, d2_w, d3_cut, d3_w, eeq_cn_cut, eeq_cap;
     const double* m_paircut2;
     int output_aes;  // 1: gradient with the AES potentials of the output moments (xtb 6.8.0)
+    // implicit solvation (crates/solvation): on, ALPB (else GBSA), model scalars, per-atom
+    // radii, surface and H-bond parameters, per-molecule SASA neighbour cutoff
+    int solv, sv_alpb;
+    double sv_keps, sv_alpbet, sv_c1, sv_lrcut, sv_w, sv_ah0, sv_ah1, sv_ah3, sv_gshift;
+    const double *sv_vdwr, *sv_rho, *sv_svdw, *sv_vdwsa, *sv_t1, *sv_t2, *sv_wrp, *sv_gam, *sv_hbmag;
+    const double* sv_srcut;
     int split;                        // 1: basis-transform and W GEMMs in split precision
 };
 
@@ -116,6 +123,11 @@ struct State {
     double* e_atom;    // natT
     double* mol_cyc;   // nmol: SM cycles of each molecule's last eigen phase (profiling runs)
     double* e_terms;   // natT*5: ES2, ES3, AES, D4 two-body, band per atom
+    // implicit solvation: Born radii and dbrad/dpsi, surface areas, H-bond weights and their
+    // surface derivative factors, self surface derivatives (natT*3), dE/dpsi, A_det per molecule,
+    // SASA neighbour lists (natT*SOLV_MAXNB) and counts
+    double *sv_brad, *sv_dbrad, *sv_sasa, *sv_hbw, *sv_dhbdw, *sv_selfg, *sv_dedbr, *sv_adet;
+    int *sv_nb, *sv_nbn;
     // cooperative scratch
     double* red;       // reduction partials (grid-size * 8)
     double* eeq_A;     // EEQ system matrices (sum (nat)^2)

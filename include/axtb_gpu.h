@@ -66,6 +66,13 @@ typedef struct AxtbOptions {
                           screening, aufbau up to 0.1 K, its EEQ-start CN, the gradient with the
                           AES potentials of the output moments), 2 tblite 0.8.0's (mctc-lib radii,
                           the same cutoffs, atom-pair integral cutoff, zero-charge start) */
+    int32_t solvation;   /* implicit solvation (crates/axtb/src/solvation.rs, crates/solvation): -1 none
+                          (default), 0 ALPB, 1 GBSA; GFN2-xTB parameters of xtb, the corrected variant in
+                          the axtb and tblite conventions, xtb's in the xtb conventions */
+    const char* solvent; /* the solvent, by xtb's names and aliases (case-insensitive); read during
+                          axtb_gpu_create / axtb_gpu_batch_create only */
+    int32_t solvation_state; /* reference state of the solvation free energy: 0 gsolv (default),
+                          1 bar1M, 2 reference */
 } AxtbOptions;
 
 /* Results of one single point (crates/base/src/method/results.rs:39-57). Array members are
