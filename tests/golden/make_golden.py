@@ -89,6 +89,9 @@ def main() -> None:
             "max_iter": c.get("max_iter", 250), "model": model, "solvent": c[model],
             "state": c.get("solvation_state") or "gsolv", "energy": ax["energy"],
             "iterations": ax.get("iterations"),
+            "conventions": {k: {"energy": r["programs"][p]["energy"], "iterations": r["programs"][p].get("iterations")}
+                            for k, p in (("xtb", "axtb[xtb]"), ("tblite", "axtb[tblite]"))
+                            if r["programs"].get(p, {}).get("ok") and "energy" in r["programs"][p]},
         })
     SOLV.write_text(json.dumps({"source": "axtb tests/reference_matrix/results.json (programs.axtb, "
                                           "category solvation)", "cases": solv}, indent=0))

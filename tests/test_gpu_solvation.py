@@ -2,7 +2,8 @@
 
 tests/golden/solvation.json: 483 solvated single points of axtb's reference matrix (ALPB and GBSA,
 25 solvents and xtb's aliases, gsolv / bar1M / reference states) with axtb's energies; every one
-must agree to 1e-9 Eh (one batch per solvent setting). Gradients against the oracle to
+must agree to 1e-9 Eh (one batch per solvent setting), in axtb's own conventions and in its xtb
+(483 recorded) and tblite (468) conventions. Gradients against the oracle to
 1e-8 Eh/bohr.
 """
 import json
@@ -16,20 +17,25 @@ pytestmark = pytest.mark.gpu
 SOLV = json.loads((Path(__file__).parent / "golden" / "solvation.json").read_text())["cases"]
 
 
-def test_solvated_energies_match_axtb_records(engine):
+@pytest.mark.parametrize("conv,count", [("axtb", 483), ("xtb", 483), ("tblite", 468)])
+def test_solvated_energies_match_axtb_records(engine, conv, count):
     groups = {}
     for c in SOLV:
-        groups.setdefault((c["model"], c["solvent"], c["state"], c["accuracy"], c["etemp"], c["max_iter"]), []).append(c)
+        if conv == "axtb" or conv in c["conventions"]:
+            key = (c["model"], c["solvent"], c["state"], c["accuracy"], c["etemp"], c["max_iter"])
+            groups.setdefault(key, []).append(c)
     bad, n = [], 0
     for (model, solvent, state, acc, etemp, max_iter), cases in groups.items():
         mols = [(np.array(c["numbers"]), np.array(c["positions"]), c["charge"], c["uhf"]) for c in cases]
-        b = engine.Batch(mols, accuracy=acc, etemp=etemp, max_iter=max_iter, solvation=(model, solvent, state))
+        b = engine.Batch(mols, accuracy=acc, etemp=etemp, max_iter=max_iter, solvation=(model, solvent, state),
+                         conventions=conv)
         for c, r in zip(cases, b.run(gradient=False)):
             n += 1
-            if r.status != 0 or abs(r.energy - c["energy"]) >= 1e-9:
-                bad.append((c["id"], r.status, r.energy - c["energy"]))
+            rec = c if conv == "axtb" else c["conventions"][conv]
+            if r.status != 0 or abs(r.energy - rec["energy"]) >= 1e-9:
+                bad.append((c["id"], r.status, r.energy - rec["energy"]))
         b.close()
-    assert n == 483 and not bad, bad[:10]
+    assert n == count and not bad, bad[:10]
 
 
 @pytest.mark.parametrize("solvation", [("alpb", "water", "gsolv"), ("gbsa", "ch2cl2", "reference"),
