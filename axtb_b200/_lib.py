@@ -36,7 +36,7 @@ class AxtbResult(C.Structure):
                 ("dipole", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)), ("dpat", C.POINTER(C.c_double)),
                 ("qpat", C.POINTER(C.c_double)), ("terms", C.c_double * 8), ("iterations", C.c_int32),
                 ("converged", C.c_int32), ("status", C.c_int32), ("energy_change", C.c_double),
-                ("residual", C.c_double), ("mixer_used", C.c_int32)]
+                ("residual", C.c_double), ("mixer_used", C.c_int32), ("solvation", C.c_double)]
 
 
 class AxtbMol(C.Structure):

@@ -76,7 +76,8 @@ class _ResultBuffers:
         r = self.res
         return SinglePoint(energy=r.energy, gradient=self.grad.copy() if gradient else None, charges=self.q.copy(),
                            dipole=self.dip.copy(), qsh=self.qsh.copy(), dpat=self.dp.copy(), qpat=self.qp.copy(),
-                           terms=dict(zip(TERM_NAMES, list(r.terms))), iterations=r.iterations,
+                           terms=dict(zip(TERM_NAMES, list(r.terms)), solvation=r.solvation),
+                           iterations=r.iterations,
                            converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
                            residual=r.residual, mixer_used=MIXER_USED[r.mixer_used])
 

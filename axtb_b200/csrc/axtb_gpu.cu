@@ -646,7 +646,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addD((size_t)nsqT * 2);
     if (o.solv >= 0) {  // solvation: 9 per-atom parameter arrays, 7 per-atom state arrays, lists
         addD((size_t)natT * 9 + nmol);
-        addD((size_t)natT * 9 + nmol);
+        addD((size_t)natT * 10 + nmol * 2);
         addI((size_t)natT * axg::SOLV_MAXNB + natT);
     }
     bytes += 1 << 20;
@@ -932,6 +932,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         s.sv_selfg = ar.take<double>((size_t)natT * 3);
         s.sv_dedbr = ar.take<double>(natT);
         s.sv_adet = ar.take<double>(nmol);
+        s.sv_eatom = ar.take<double>(natT);
+        s.sv_emol = ar.take<double>(nmol);
         s.sv_nb = ar.take<int>((size_t)natT * axg::SOLV_MAXNB);
         s.sv_nbn = ar.take<int>(natT);
     }

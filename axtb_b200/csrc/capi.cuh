@@ -19,6 +19,8 @@ static int status_code(int bits, int conv) {
 void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     vector<double> eel(nmol), erep(nmol), eatm(nmol), terms((size_t)nmol * 8), de(nmol), res(nmol);
     vector<int> st_(nmol), conv(nmol), nit(nmol), nit0(nmol), used(nmol);
+    vector<double> esolv(nmol, 0.0);
+    if (B.solv) CK(cudaMemcpyAsync(esolv.data(), S.sv_emol, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
     vector<double> grad((size_t)natT * 3), qat(natT), dp((size_t)natT * 3), qp((size_t)natT * 6), qsh(nshT);
     CK(cudaMemcpyAsync(eel.data(), S.energy, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(erep.data(), S.e_fixed, sizeof(double) * nmol, cudaMemcpyDeviceToHost, st));
@@ -51,6 +53,7 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
         r.iterations = conv[m] ? nit[m] : nit[m] + nit0[m];
         r.converged = conv[m];
         r.mixer_used = used[m];
+        r.solvation = esolv[m];
         r.energy_change = de[m];
         r.residual = res[m];
         r.status = status_code(st_[m], conv[m]);

@@ -127,6 +127,7 @@ struct State {
     // surface derivative factors, self surface derivatives (natT*3), dE/dpsi, A_det per molecule,
     // SASA neighbour lists (natT*SOLV_MAXNB) and counts
     double *sv_brad, *sv_dbrad, *sv_sasa, *sv_hbw, *sv_dhbdw, *sv_selfg, *sv_dedbr, *sv_adet;
+    double *sv_eatom, *sv_emol;  // solvation energy per atom (last iteration) and per molecule
     int *sv_nb, *sv_nbn;
     // cooperative scratch
     double* red;       // reduction partials (grid-size * 8)

@@ -343,6 +343,12 @@ __device__ bool scf_iteration_end(const Batch& B, const State& S, int m) {
         tb += S.e_terms[5 * (a0 + a) + 4];
     }
     e = cta_sum(e) + S.ts[m];
+    if (B.solv) {  // the solvation term (crates/axtb/src/calculator.rs:314)
+        double es = 0.0;
+        for (int a = tid; a < nat; a += nthr) es += S.sv_eatom[a0 + a];
+        es = cta_sum(es);
+        if (tid == 0) S.sv_emol[m] = es;
+    }
     t2 = cta_sum(t2);
     t3 = cta_sum(t3);
     ta = cta_sum(ta);

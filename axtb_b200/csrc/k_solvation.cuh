@@ -283,7 +283,9 @@ __global__ void k_solv_energy(Batch B, State S) {
     double v = born_row(B, S, a, mv, S.qat_out, lane);
     if (lane == 0) {
         double q = S.qat_out[a];
-        S.e_atom[a] += q * (0.5 * v) + S.sv_sasa[a] * B.sv_gam[a] + B.sv_gshift / mv.n;
+        double e = q * (0.5 * v) + S.sv_sasa[a] * B.sv_gam[a] + B.sv_gshift / mv.n;
+        S.e_atom[a] += e;
+        S.sv_eatom[a] = e;
     }
 }
 

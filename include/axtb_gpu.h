@@ -94,6 +94,8 @@ typedef struct AxtbResult {
     double residual;        /* last residual norm (ScfNotConverged payload) */
     int32_t mixer_used;     /* mixer of the result (ScfResult::mixer_used): 0 Broyden, 1 DIIS,
                                2 DIIS after Broyden did not converge ("diis-fallback") */
+    double solvation;       /* the solvation term (surface, shift and polar parts; part of the
+                               electronic subtotal as in crates/axtb/src/calculator.rs:301-316); 0 without */
 } AxtbResult;
 
 /* One molecule of a batch: atomic numbers, positions (bohr, nat*3 row-major), charge and the

@@ -2492,6 +2492,7 @@ int run(OracleRun* R) {
     Moments out;
     bool converged = false;
     int iters = 0, iters_all = 0;
+    double esolv_last = 0.0;
     vector<double> packed, q_last;  // q_last: the last input of the last attempt
     // the attempts of the mixer plan (crates/axtb/src/scf/mixing.rs:163-199, run by
     // crates/axtb/src/xtb.rs:590-645): auto = Broyden, then DIIS from the start guess with its own
@@ -2618,6 +2619,7 @@ int run(OracleRun* R) {
             double band = 0.0;
             for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
             double esolv = solv ? solv_energy(sv, out.qat) : 0.0;
+            esolv_last = esolv;
             double energy = e2 + e3 + eaes + edisp + ts + band + esolv;
             if (!std::isfinite(energy)) throw Fail(4, "non-finite energy");
             double res = 0.0;
@@ -2647,6 +2649,7 @@ int run(OracleRun* R) {
     terms[0] = e_rep;
     terms[1] += e_atm;
     double energy = e_rep + e_atm + terms[2] + e_solv_fixed;
+    R->e_solvation = e_solv_fixed + esolv_last;
     if (R->energy) *R->energy = energy;
     if (R->terms) std::memcpy(R->terms, terms, sizeof terms);
     if (R->qat) std::copy(out.qat.begin(), out.qat.end(), R->qat);
@@ -2788,6 +2791,7 @@ extern "C" int oracle_singlepoint(OracleRun* R) {
     R->iterations = 0;
     R->converged = 0;
     R->mixer_used = 0;
+    R->e_solvation = 0.0;
     try {
         return run(R);
     } catch (const Fail& f) {

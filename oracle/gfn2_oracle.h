@@ -47,6 +47,7 @@ typedef struct {
     double* focc;            /* nao occupations */
     double* density;         /* nao*nao, column-major */
     double* wdensity;        /* nao*nao */
+    double e_solvation;      /* the solvation term (its surface, shift and polar parts), Eh */
     int iterations;          /* of the converged attempt; of all attempts when none converged */
     int converged;
     int mixer_used;          /* mixer of the last attempt: 0 Broyden, 1 DIIS, 2 DIIS after Broyden (auto) */

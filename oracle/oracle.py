@@ -31,7 +31,7 @@ class _Run(C.Structure):
         ("dipole", C.POINTER(C.c_double)), ("terms", C.POINTER(C.c_double)),
         ("emo", C.POINTER(C.c_double)), ("focc", C.POINTER(C.c_double)),
         ("density", C.POINTER(C.c_double)), ("wdensity", C.POINTER(C.c_double)),
-        ("iterations", C.c_int), ("converged", C.c_int), ("mixer_used", C.c_int), ("nsh", C.c_int),
+        ("e_solvation", C.c_double), ("iterations", C.c_int), ("converged", C.c_int), ("mixer_used", C.c_int), ("nsh", C.c_int),
         ("nao", C.c_int),
         ("error", C.c_char * 256),
     ]
@@ -156,6 +156,7 @@ def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=30
     out["mixer_used"] = MIXER_USED[r.mixer_used]
     out["energy"] = float(out["energy"][0])
     out["terms"] = dict(zip(TERM_NAMES, out["terms"].tolist()))
+    out["terms"]["solvation"] = r.e_solvation
     out["iterations"] = r.iterations
     out["converged"] = bool(r.converged)
     if matrices:

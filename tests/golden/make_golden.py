@@ -88,7 +88,7 @@ def main() -> None:
             "uhf": c["uhf"], "accuracy": c.get("accuracy", 1.0), "etemp": c.get("etemp", 300.0),
             "max_iter": c.get("max_iter", 250), "model": model, "solvent": c[model],
             "state": c.get("solvation_state") or "gsolv", "energy": ax["energy"],
-            "iterations": ax.get("iterations"),
+            "iterations": ax.get("iterations"), "solvation_term": (ax.get("terms") or {}).get("solvation"),
             "conventions": {k: {"energy": r["programs"][p]["energy"], "iterations": r["programs"][p].get("iterations")}
                             for k, p in (("xtb", "axtb[xtb]"), ("tblite", "axtb[tblite]"))
                             if r["programs"].get(p, {}).get("ok") and "energy" in r["programs"][p]},

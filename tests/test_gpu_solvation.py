@@ -34,6 +34,8 @@ def test_solvated_energies_match_axtb_records(engine, conv, count):
             rec = c if conv == "axtb" else c["conventions"][conv]
             if r.status != 0 or abs(r.energy - rec["energy"]) >= 1e-9:
                 bad.append((c["id"], r.status, r.energy - rec["energy"]))
+            if conv == "axtb" and abs(r.terms["solvation"] - c["solvation_term"]) >= 1e-9:
+                bad.append((c["id"], "solvation term", r.terms["solvation"] - c["solvation_term"]))
         b.close()
     assert n == count and not bad, bad[:10]
 
@@ -52,6 +54,7 @@ def test_solvated_singlepoint_matches_oracle(engine, golden, solvation, cid):
     assert abs(r.energy - ref["energy"]) < 1e-9, (r.energy, ref["energy"])
     assert np.abs(r.gradient - ref["gradient"]).max() < 1e-8
     assert np.abs(r.charges - ref["qat"]).max() < 1e-7
+    assert abs(r.terms["solvation"] - ref["terms"]["solvation"]) < 1e-9
 
 
 def test_unknown_solvent_is_an_input_error(engine):

@@ -43,6 +43,18 @@ def test_solvated_energies_match_axtb_records(conv, count):
                                                          for s in ("gsolv", "bar1M", "reference")}
 
 
+def test_solvation_term_matches_axtb_records():
+    """The reported solvation term (surface, shift and polar parts; crates/axtb/src/calculator.rs:314)."""
+    worst = 0.0
+    for c in SOLV:
+        r = O.singlepoint(c["numbers"], c["positions"], c["charge"], c["uhf"], c["accuracy"], c["etemp"],
+                          c["max_iter"], gradient=False, solvation=(c["model"], c["solvent"], c["state"]))
+        worst = max(worst, abs(r["terms"]["solvation"] - c["solvation_term"]))
+    assert worst < 1e-9, worst
+    r = O.singlepoint([8, 1, 1], [[0, 0, 0], [0, 1.4, 1.1], [0, -1.4, 1.1]], gradient=False)
+    assert r["terms"]["solvation"] == 0.0
+
+
 @pytest.mark.parametrize("solvation", [("alpb", "water", "gsolv"), ("gbsa", "water", "bar1M"),
                                        ("alpb", "ch2cl2", "reference")])
 def test_solvated_gradient_finite_differences(golden, solvation):
