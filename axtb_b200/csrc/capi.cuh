@@ -39,7 +39,8 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     CK(cudaMemcpyAsync(qsh.data(), S.qsh_out, sizeof(double) * nshT, cudaMemcpyDeviceToHost, st));
     if (want_grad) CK(cudaMemcpyAsync(grad.data(), S.grad, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    d2h_bytes += (long long)(sizeof(double) * (nmol * 14 + (size_t)natT * 10 + nshT) + sizeof(int) * nmol * 5) +
+    d2h_bytes += (long long)(sizeof(double) * (nmol * (B.solv ? 15 : 14) + (size_t)natT * 10 + nshT) +
+                             sizeof(int) * nmol * 5) +
                  (want_grad ? (long long)sizeof(double) * natT * 3 : 0);
     for (int m = 0; m < nmol; m++) {
         AxtbResult& r = outs[m];
