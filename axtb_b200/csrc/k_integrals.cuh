@@ -297,12 +297,50 @@ __global__ void k_h0_gradient(Batch B, State S, const long long* m_pair0, long l
             if (pair_screened(B.s_amin[si], B.s_amin[sj], r2, B.intcut)) continue;
             load_shell(B, sj, cj);
             int li_ = ci.l, lj_ = cj.l, ncj = ncart(lj_), nci = ncart(li_);
-            // Cartesian values [s, d_j(3), m_j(6)] and their R_i derivatives (moments about R_j)
-            double val[36][10], der[36][30];
-            for (int p = 0; p < ncj * nci; p++) {
-                for (int x = 0; x < 10; x++) val[p][x] = 0.0;
-                for (int x = 0; x < 30; x++) der[p][x] = 0.0;
-            }
+            // shell-pair factors of H0
+            double shpi = 1.0 + B.s_shpoly[si] * rr, shpj = 1.0 + B.s_shpoly[sj] * rr;
+            double shp = shpi * shpj;
+            double dshp = (shpi * B.s_shpoly[sj] + shpj * B.s_shpoly[si]) * 0.5 * rr / r2;
+            double dsv[3] = {dshp / shp * vec[0], dshp / shp * vec[1], dshp / shp * vec[2]};
+            double hs = hscale(B, sj, ja, si, ia) * shp;
+            double hij = 0.5 * (S.se[si] + S.se[sj]) * hs;
+            double dhdcni = S.dsedcn[si] * hs, dhdcnj = S.dsedcn[sj] * hs;
+            // The contraction is linear in the integrals of each AO pair, and its multipole part
+            // uses the same potentials for all of them: the spherical transform moves onto three
+            // Cartesian weights (P, the overlap-derivative factor, 2 P h), so the integrals are
+            // accumulated as they are made instead of held per Cartesian pair.
+            double wp[36], ws[36], wh[36];
+            for (int c = 0; c < nci * ncj; c++) wp[c] = ws[c] = wh[c] = 0.0;
+            int nsj = nsph(lj_);
+            for (int im = 0; im < nsph(li_); im++)
+                for (int jm = 0; jm < nsj; jm++) {
+                    int mu = B.s_ao0[sj] + jm - ao0, nu = B.s_ao0[si] + im - ao0;
+                    long long e1 = mat + mu + (long long)nu * n;
+                    double pij = S.P[e1], hpij = pij * hij;
+                    int amu = B.s_ao0[sj] + jm, anu = B.s_ao0[si] + im;
+                    double vmu = S.vsh[B.o_sh[amu]] + S.vat[B.o_at[amu]];
+                    double vnu = S.vsh[B.o_sh[anu]] + S.vat[B.o_at[anu]];
+                    double sval = -pij * (vmu + vnu) + 2.0 * hpij - 2.0 * S.W[e1];
+                    for (int ic = 0; ic < nci; ic++) {
+                        double ti = sph_t(li_, im, ic);
+                        if (ti == 0.0) continue;
+                        for (int jc = 0; jc < ncj; jc++) {
+                            double tj = sph_t(lj_, jm, jc);
+                            if (tj == 0.0) continue;
+                            double f = tj * ti;
+                            int c = jc + ncj * ic;
+                            wp[c] += f * pij;
+                            ws[c] += f * sval;
+                            wh[c] += f * (2.0 * hpij);
+                        }
+                    }
+                }
+            // weighted Cartesian values [s, d_j(3), m_j(6)] and R_i derivatives (moments about R_j):
+            // av, ad with the P weights; sds = the overlap derivative with its factor; sh = the
+            // overlap with 2 P h
+            double av[10], ad[30], sds[3] = {0.0, 0.0, 0.0}, sh = 0.0;
+            for (int x = 0; x < 10; x++) av[x] = 0.0;
+            for (int x = 0; x < 30; x++) ad[x] = 0.0;
             double t[3][6][6];
             for (int ip = 0; ip < ci.np; ip++) {
                 double ai2 = 2.0 * ci.a[ip];
@@ -315,6 +353,8 @@ __global__ void k_h0_gradient(Batch B, State S, const long long* m_pair0, long l
                         int ea[3];
                         cart_exp(li_, ic, ea);
                         for (int jc = 0; jc < ncj; jc++) {
+                            int c = jc + ncj * ic;
+                            double fp = cc * wp[c], fs = cc * ws[c], fh = cc * wh[c];
                             int eb[3];
                             cart_exp(lj_, jc, eb);
                             double v[3][3], gg[3][3];
@@ -325,82 +365,58 @@ __global__ void k_h0_gradient(Batch B, State S, const long long* m_pair0, long l
                                     if (ea[k] > 0) x -= ea[k] * t[k][ea[k] - 1][eb[k] + mm];
                                     gg[k][mm] = x;
                                 }
-                            double* vc = val[jc + ncj * ic];
-                            double* dc = der[jc + ncj * ic];
                             for (int nq = 0; nq < 10; nq++) {
                                 double X = v[0][MOM[nq][0]], Y = v[1][MOM[nq][1]], Zz = v[2][MOM[nq][2]];
-                                vc[nq] += cc * X * Y * Zz;
-                                dc[3 * nq] += cc * gg[0][MOM[nq][0]] * Y * Zz;
-                                dc[3 * nq + 1] += cc * X * gg[1][MOM[nq][1]] * Zz;
-                                dc[3 * nq + 2] += cc * X * Y * gg[2][MOM[nq][2]];
+                                double d0 = gg[0][MOM[nq][0]] * Y * Zz, d1 = X * gg[1][MOM[nq][1]] * Zz;
+                                double d2 = X * Y * gg[2][MOM[nq][2]], xyz = X * Y * Zz;
+                                av[nq] += fp * xyz;
+                                ad[3 * nq] += fp * d0;
+                                ad[3 * nq + 1] += fp * d1;
+                                ad[3 * nq + 2] += fp * d2;
+                                if (nq == 0) {
+                                    sds[0] += fs * d0;
+                                    sds[1] += fs * d1;
+                                    sds[2] += fs * d2;
+                                    sh += fh * xyz;
+                                }
                             }
                         }
                     }
                 }
             }
-            double shpi = 1.0 + B.s_shpoly[si] * rr, shpj = 1.0 + B.s_shpoly[sj] * rr;
-            double shp = shpi * shpj;
-            double dshp = (shpi * B.s_shpoly[sj] + shpj * B.s_shpoly[si]) * 0.5 * rr / r2;
-            double dsv[3] = {dshp / shp * vec[0], dshp / shp * vec[1], dshp / shp * vec[2]};
-            double hs = hscale(B, sj, ja, si, ia) * shp;
-            double hij = 0.5 * (S.se[si] + S.se[sj]) * hs;
-            double dhdcni = S.dsedcn[si] * hs, dhdcnj = S.dsedcn[sj] * hs;
-            int nsj = nsph(lj_);
-            for (int im = 0; im < nsph(li_); im++)
-                for (int jm = 0; jm < nsj; jm++) {
-                    double sv[10], sd[30];
-                    for (int x = 0; x < 10; x++) sv[x] = 0.0;
-                    for (int x = 0; x < 30; x++) sd[x] = 0.0;
-                    for (int ic = 0; ic < nci; ic++) {
-                        double ti = sph_t(li_, im, ic);
-                        if (ti == 0.0) continue;
-                        for (int jc = 0; jc < ncj; jc++) {
-                            double tj = sph_t(lj_, jm, jc);
-                            if (tj == 0.0) continue;
-                            double f = tj * ti;
-                            for (int x = 0; x < 10; x++) sv[x] += f * val[jc + ncj * ic][x];
-                            for (int x = 0; x < 30; x++) sd[x] += f * der[jc + ncj * ic][x];
-                        }
-                    }
-                    double s = sv[0];
-                    double djv[3] = {sv[1], sv[2], sv[3]};
-                    double ds[3] = {sd[0], sd[1], sd[2]};
-                    double ddj[3][3], dmj[3][6], ddi[3][3], dmi[3][6];
-                    for (int k = 0; k < 3; k++) {
-                        for (int c = 0; c < 3; c++) ddj[k][c] = sd[3 * (1 + c) + k];
-                        for (int c = 0; c < 6; c++) dmj[k][c] = sd[3 * (4 + c) + k];
-                    }
-                    for (int k = 0; k < 3; k++) {
-                        for (int c = 0; c < 3; c++) ddi[k][c] = ddj[k][c] - vec[c] * ds[k];
-                        ddi[k][k] -= s;
-                        for (int nq = 0; nq < 6; nq++) {
-                            int a_ = AB[nq][0], b_ = AB[nq][1];
-                            double x = dmj[k][nq] - vec[a_] * ddj[k][b_] - vec[b_] * ddj[k][a_] + vec[a_] * vec[b_] * ds[k];
-                            if (a_ == k) x += -djv[b_] + vec[b_] * s;
-                            if (b_ == k) x += -djv[a_] + vec[a_] * s;
-                            dmi[k][nq] = x;
-                        }
-                    }
-                    for (int k = 0; k < 3; k++) {
-                        traceless6(dmi[k]);
-                        traceless6(dmj[k]);
-                    }
-                    int mu = B.s_ao0[sj] + jm - ao0, nu = B.s_ao0[si] + im - ao0;
-                    long long e1 = mat + mu + (long long)nu * n;
-                    double pij = S.P[e1], hpij = pij * hij;
-                    int amu = B.s_ao0[sj] + jm, anu = B.s_ao0[si] + im;
-                    double vmu = S.vsh[B.o_sh[amu]] + S.vat[B.o_at[amu]];
-                    double vnu = S.vsh[B.o_sh[anu]] + S.vat[B.o_at[anu]];
-                    double sval = -pij * (vmu + vnu) + 2.0 * hpij - 2.0 * S.W[e1];
-                    for (int k = 0; k < 3; k++) {
-                        double mp = 0.0;
-                        for (int c = 0; c < 3; c++) mp += ddi[k][c] * vdi[c] + ddj[k][c] * vdj[c];
-                        for (int c = 0; c < 6; c++) mp += dmi[k][c] * vqi[c] + dmj[k][c] * vqj[c];
-                        dg[k] += sval * ds[k] + 2.0 * hpij * s * dsv[k] - pij * mp;
-                    }
-                    dcni += dhdcni * pij * s;
-                    dcnj += dhdcnj * pij * s;
+            // the multipole part: moments about R_i from those about R_j, traceless quadrupoles,
+            // contracted with the atomic dipole and quadrupole potentials
+            double s = av[0];
+            double djv[3] = {av[1], av[2], av[3]};
+            double ds[3] = {ad[0], ad[1], ad[2]};
+            double ddj[3][3], dmj[3][6], ddi[3][3], dmi[3][6];
+            for (int k = 0; k < 3; k++) {
+                for (int c = 0; c < 3; c++) ddj[k][c] = ad[3 * (1 + c) + k];
+                for (int c = 0; c < 6; c++) dmj[k][c] = ad[3 * (4 + c) + k];
+            }
+            for (int k = 0; k < 3; k++) {
+                for (int c = 0; c < 3; c++) ddi[k][c] = ddj[k][c] - vec[c] * ds[k];
+                ddi[k][k] -= s;
+                for (int nq = 0; nq < 6; nq++) {
+                    int a_ = AB[nq][0], b_ = AB[nq][1];
+                    double x = dmj[k][nq] - vec[a_] * ddj[k][b_] - vec[b_] * ddj[k][a_] + vec[a_] * vec[b_] * ds[k];
+                    if (a_ == k) x += -djv[b_] + vec[b_] * s;
+                    if (b_ == k) x += -djv[a_] + vec[a_] * s;
+                    dmi[k][nq] = x;
                 }
+            }
+            for (int k = 0; k < 3; k++) {
+                traceless6(dmi[k]);
+                traceless6(dmj[k]);
+            }
+            for (int k = 0; k < 3; k++) {
+                double mp = 0.0;
+                for (int c = 0; c < 3; c++) mp += ddi[k][c] * vdi[c] + ddj[k][c] * vdj[c];
+                for (int c = 0; c < 6; c++) mp += dmi[k][c] * vqi[c] + dmj[k][c] * vqj[c];
+                dg[k] += sds[k] + sh * dsv[k] - mp;
+            }
+            dcni += dhdcni * s;
+            dcnj += dhdcnj * s;
         }
     }
     o[0] = dg[0];
