@@ -24,3 +24,23 @@ def test_invalid_options_are_input_errors(opts):
                                   dict(solvation=("ALPB", "dichloromethane", "reference"))])
 def test_valid_options_create(opts):
     A.Calculator([8, 1, 1], **opts).close()
+
+
+@pytest.mark.parametrize("numbers,kw,kind", [
+    ([8, 1, 1], dict(uhf=1), "input"),              # unpaired electrons of the wrong parity
+    ([1], dict(charge=2.0), "input"),               # a negative electron count
+    ([1, 1], dict(uhf=4), "input"),                 # more unpaired electrons than electrons
+    ([8, 1, 1], dict(charge=0.5), "input"),         # fractional electron counts
+    ([87], {}, "unsupported_element"),              # beyond GFN2-xTB's elements
+    ([], {}, "input"),                              # no atoms
+])
+def test_molecule_checks(numbers, kw, kind):
+    """crates/base/src/molecule.rs:35-99 and the electron count of crates/axtb/src/xtb.rs:1178-1212,
+    checked when the handle is created."""
+    with pytest.raises(A.AxtbError) as e:
+        A.Calculator(numbers, **kw)
+    assert e.value.kind == kind
+
+
+def test_heaviest_element_is_accepted():
+    A.Calculator([86]).close()
