@@ -6,5 +6,5 @@ workloads; ``torch_ops`` exposes the batched energy to PyTorch; ``hessian`` give
 semi-numerical Hessian from one batch of displaced gradients; ``sharding`` spreads molecules
 over GPUs.
 """
-from .calculator import AxtbError, Batch, Calculator, SinglePoint, basis_size  # noqa: F401
+from .calculator import AxtbError, Batch, Calculator, Moments, SinglePoint, basis_size  # noqa: F401
 from .hessian import Hessian, numerical_hessian  # noqa: F401

@@ -28,7 +28,7 @@ class AxtbOptions(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("etemp", C.c_double), ("max_iter", C.c_int32), ("damping", C.c_double),
                 ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("mixer", C.c_int32),
                 ("conventions", C.c_int32), ("solvation", C.c_int32), ("solvent", C.c_char_p),
-                ("solvation_state", C.c_int32)]
+                ("solvation_state", C.c_int32), ("dispersion", C.c_int32)]
 
 
 class AxtbResult(C.Structure):
@@ -36,7 +36,10 @@ class AxtbResult(C.Structure):
                 ("dipole", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)), ("dpat", C.POINTER(C.c_double)),
                 ("qpat", C.POINTER(C.c_double)), ("terms", C.c_double * 8), ("iterations", C.c_int32),
                 ("converged", C.c_int32), ("status", C.c_int32), ("energy_change", C.c_double),
-                ("residual", C.c_double), ("mixer_used", C.c_int32), ("solvation", C.c_double)]
+                ("residual", C.c_double), ("mixer_used", C.c_int32), ("solvation", C.c_double),
+                ("emo", C.POINTER(C.c_double)), ("focc", C.POINTER(C.c_double)), ("focc_alpha", C.POINTER(C.c_double)),
+                ("fermi_levels", C.c_double * 2), ("electronic_temperature", C.c_double), ("nao", C.c_int32),
+                ("warm_start", C.c_int32), ("fallback_iterations", C.c_int32), ("timings", C.c_double * 4)]
 
 
 class AxtbMol(C.Structure):
@@ -68,6 +71,10 @@ SIGNATURES = {
     "axtb_gpu_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "axtb_gpu_batch_set_restart": (C.c_int, [C.c_void_p, C.c_int32]),
     "axtb_gpu_batch_profile": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "axtb_gpu_get_moments": (C.c_int, [C.c_void_p, PD, PD, PD]),
+    "axtb_gpu_set_moments": (C.c_int, [C.c_void_p, PD, PD, PD, C.c_int32]),
+    "axtb_gpu_batch_get_moments": (C.c_int, [C.c_void_p, C.c_int32, PD, PD, PD]),
+    "axtb_gpu_batch_set_moments": (C.c_int, [C.c_void_p, C.c_int32, PD, PD, PD]),
 }
 
 _lib = None

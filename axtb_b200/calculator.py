@@ -44,10 +44,42 @@ class SinglePoint:
     energy_change: float = 0.0
     residual: float = 0.0
     mixer_used: str = "broyden"  # "broyden", "diis" or "diis-fallback" (auto after Broyden failed)
+    # the electronic structure (with levels=True): every orbital energy, the occupations of both
+    # spins and of the alpha spin, the Fermi levels (NaN: aufbau filling) and the temperature
+    emo: np.ndarray | None = None
+    focc: np.ndarray | None = None
+    focc_alpha: np.ndarray | None = None
+    fermi_levels: tuple = (float("nan"), float("nan"))
+    electronic_temperature: float = 0.0
+    start: str = "guess"        # "previous": started from previous or given moments (ScfReport::start)
+    attempts: list = field(default_factory=list)  # [(mixer, iterations, converged)] of the plan
+    timings: dict = field(default_factory=dict)   # wall time (s) per phase of the device pass
 
 
 def _ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+@dataclass
+class Moments:
+    """SCC moments of one molecule (axtb's ScfGuess / ScfData): shell charges, atomic dipoles
+    and atomic quadrupoles (xx, xy, yy, xz, yz, zz)."""
+    qsh: np.ndarray
+    dpat: np.ndarray
+    qpat: np.ndarray
+
+    @staticmethod
+    def empty(nat: int, nsh: int) -> "Moments":
+        return Moments(np.zeros(nsh), np.zeros((nat, 3)), np.zeros((nat, 6)))
+
+    def checked(self, nat: int, nsh: int) -> "Moments":
+        w = Moments(np.ascontiguousarray(self.qsh, dtype=np.float64).reshape(-1),
+                    np.ascontiguousarray(self.dpat, dtype=np.float64).reshape(-1, 3),
+                    np.ascontiguousarray(self.qpat, dtype=np.float64).reshape(-1, 6))
+        if w.qsh.size != nsh or w.dpat.shape[0] != nat or w.qpat.shape[0] != nat:
+            raise AxtbError(1, f"moments of {w.qsh.size} shells and {w.dpat.shape[0]} atoms for a molecule of "
+                               f"{nsh} shells and {nat} atoms")
+        return w
 
 
 def basis_size(numbers):
@@ -60,26 +92,53 @@ def basis_size(numbers):
 
 
 class _ResultBuffers:
-    def __init__(self, nat, nsh):
+    def __init__(self, nat, nsh, nao=0):
         self.grad = np.zeros((nat, 3))
         self.q = np.zeros(nat)
         self.dip = np.zeros(3)
         self.qsh = np.zeros(nsh)
         self.dp = np.zeros((nat, 3))
         self.qp = np.zeros((nat, 6))
+        self.nao = nao
+        self.emo, self.focc, self.focca = np.zeros(nao), np.zeros(nao), np.zeros(nao)
         self.res = _lib.AxtbResult()
+        self.bind(False)
+
+    def bind(self, levels: bool):
+        """Point the result at these buffers (the level arrays only when levels are wanted: they
+        cost the engine one more pass and their copy back)."""
         r = self.res
         r.gradient, r.charges, r.dipole = _ptr(self.grad), _ptr(self.q), _ptr(self.dip)
         r.qsh, r.dpat, r.qpat = _ptr(self.qsh), _ptr(self.dp), _ptr(self.qp)
+        on = levels and self.nao > 0
+        r.emo = _ptr(self.emo) if on else None
+        r.focc = _ptr(self.focc) if on else None
+        r.focc_alpha = _ptr(self.focca) if on else None
+        self.levels = on
+        return r
 
     def result(self, gradient: bool) -> SinglePoint:
         r = self.res
+        used = MIXER_USED[r.mixer_used]
+        if used == "diis-fallback":
+            attempts = [("broyden", r.fallback_iterations, False), ("diis", r.iterations if r.converged else
+                                                                    r.iterations - r.fallback_iterations,
+                                                                    bool(r.converged))]
+        else:
+            attempts = [(used, r.iterations, bool(r.converged))]
         return SinglePoint(energy=r.energy, gradient=self.grad.copy() if gradient else None, charges=self.q.copy(),
                            dipole=self.dip.copy(), qsh=self.qsh.copy(), dpat=self.dp.copy(), qpat=self.qp.copy(),
                            terms=dict(zip(TERM_NAMES, list(r.terms)), solvation=r.solvation),
                            iterations=r.iterations,
                            converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
-                           residual=r.residual, mixer_used=MIXER_USED[r.mixer_used])
+                           residual=r.residual, mixer_used=used,
+                           emo=self.emo.copy() if self.levels else None,
+                           focc=self.focc.copy() if self.levels else None,
+                           focc_alpha=self.focca.copy() if self.levels else None,
+                           fermi_levels=(r.fermi_levels[0], r.fermi_levels[1]),
+                           electronic_temperature=r.electronic_temperature,
+                           start="previous" if r.warm_start else "guess", attempts=attempts,
+                           timings=dict(zip(("setup", "scf", "gradient", "total"), list(r.timings))))
 
 
 # SCC mixers by name (crates/axtb/src/scf/mixing.rs:202-214: case-insensitive, "pulay" = DIIS;
@@ -122,13 +181,13 @@ def _solvation(spec):
 
 
 def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0,
-             mixer=None, conventions="axtb", solvation=None):
+             mixer=None, conventions="axtb", solvation=None, dispersion=True):
     model, solvent, state = _solvation(solvation)
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
                                 damping=float(damping), guess=0 if guess == "eeq" else 1,
                                 precision={"fp64": 0, "split": 1}[precision], device=int(device),
                                 mixer=_mixer(mixer), conventions=_conventions(conventions), solvation=model,
-                                solvent=solvent, solvation_state=state)
+                                solvent=solvent, solvation_state=state, dispersion=1 if dispersion else 0)
 
 
 class Calculator:
@@ -146,16 +205,45 @@ class Calculator:
         if rc != 0:
             raise AxtbError(rc, _lib.last_error(None))
         self._h = h
-        self._buf = _ResultBuffers(self.nat, self.nsh)
+        self._buf = _ResultBuffers(self.nat, self.nsh, self.nao)
         self.positions = None if positions is None else np.asarray(positions, dtype=np.float64).reshape(-1, 3)
 
-    def singlepoint(self, positions=None, gradient=True) -> SinglePoint:
+    def singlepoint(self, positions=None, gradient=True, levels=True) -> SinglePoint:
+        """Energy (+ gradient) at `positions`; `levels`: also every orbital energy and the
+        occupations."""
         x = self.positions if positions is None else np.asarray(positions, dtype=np.float64).reshape(-1, 3)
         x = np.ascontiguousarray(x)
-        rc = _lib.load().axtb_gpu_singlepoint(self._h, _ptr(x), int(bool(gradient)), C.byref(self._buf.res))
+        res = self._buf.bind(levels)
+        rc = _lib.load().axtb_gpu_singlepoint(self._h, _ptr(x), int(bool(gradient)), C.byref(res))
         if rc != 0:
             raise AxtbError(rc, _lib.last_error(self._h))
         return self._buf.result(gradient)
+
+    def wavefunction(self) -> Moments | None:
+        """The moments the next SCF starts from (Method::wavefunction): the last converged
+        single point's, or given ones; None when there are none."""
+        w = Moments.empty(self.nat, self.nsh)
+        rc = _lib.load().axtb_gpu_get_moments(self._h, _ptr(w.qsh), _ptr(w.dpat), _ptr(w.qpat))
+        return w if rc == 0 else None
+
+    def set_wavefunction(self, moments: Moments):
+        """Start the next SCF from `moments` (Method::set_wavefunction)."""
+        self._set(moments, 1)
+
+    def set_history(self, moments: Moments | None):
+        """`moments` as this calculator's previous ones, None to forget them
+        (Method::set_history)."""
+        self._set(moments, 0)
+
+    def _set(self, moments, given):
+        lib = _lib.load()
+        if moments is None:
+            rc = lib.axtb_gpu_set_moments(self._h, None, None, None, given)
+        else:
+            w = moments.checked(self.nat, self.nsh)
+            rc = lib.axtb_gpu_set_moments(self._h, _ptr(w.qsh), _ptr(w.dpat), _ptr(w.qpat), given)
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(self._h))
 
     def close(self):
         if getattr(self, "_h", None):
@@ -197,15 +285,16 @@ class Batch:
         self._b = b
         self.nmol = len(molecules)
         self.natoms = np.array([len(z) for z, _ in self.mols])
-        self._bufs = [_ResultBuffers(len(z), basis_size(z)[0]) for z, _ in self.mols]
+        self._bufs = [_ResultBuffers(len(z), *basis_size(z)) for z, _ in self.mols]
         self._res = (_lib.AxtbResult * self.nmol)()
 
-    def run(self, positions=None, gradient=True):
+    def run(self, positions=None, gradient=True, levels=False):
         """Single points of every molecule (positions: list of (nat, 3) arrays or None for the
-        set-up geometries); returns a list of SinglePoint (status per molecule)."""
+        set-up geometries); returns a list of SinglePoint (status per molecule). `levels`: also
+        every orbital energy and the occupations of each molecule."""
         lib = _lib.load()
         for i, bf in enumerate(self._bufs):
-            self._res[i] = bf.res
+            self._res[i] = bf.bind(levels)
         st = np.zeros(self.nmol, dtype=np.int32)
         xp = None
         if positions is not None:
@@ -231,11 +320,30 @@ class Batch:
             raise AxtbError(rc, _lib.last_error(None))
         return st
 
-    def set_restart(self, enable: bool = True):
+    def set_restart(self, enable: bool = True, retry_fresh: bool = True):
         """Start later runs from each molecule's converged moments of the previous run (a
         trajectory of geometries); a molecule that then does not converge runs once more from
-        the guess (axtb's Calculator under Restart::Previous)."""
-        rc = _lib.load().axtb_gpu_batch_set_restart(self._b, int(bool(enable)))
+        the guess (axtb's Calculator under Restart::Previous), unless ``retry_fresh`` is False
+        (then it reports the failure, as a displaced point of axtb's numerical Hessian does)."""
+        mode = (1 if retry_fresh else 2) if enable else 0
+        rc = _lib.load().axtb_gpu_batch_set_restart(self._b, mode)
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+
+    def get_moments(self, mol: int) -> Moments:
+        """Molecule `mol`'s converged output moments of the last run."""
+        z, _ = self.mols[mol]
+        w = Moments.empty(len(z), basis_size(z)[0])
+        rc = _lib.load().axtb_gpu_batch_get_moments(self._b, mol, _ptr(w.qsh), _ptr(w.dpat), _ptr(w.qpat))
+        if rc != 0:
+            raise AxtbError(rc, _lib.last_error(None))
+        return w
+
+    def set_moments(self, mol: int, moments: Moments):
+        """Start molecule `mol` of the next run from `moments` (turns restarts on)."""
+        z, _ = self.mols[mol]
+        w = moments.checked(len(z), basis_size(z)[0])
+        rc = _lib.load().axtb_gpu_batch_set_moments(self._b, mol, _ptr(w.qsh), _ptr(w.dpat), _ptr(w.qpat))
         if rc != 0:
             raise AxtbError(rc, _lib.last_error(None))
 

@@ -239,6 +239,7 @@ struct Opt {
     int solv = -1;        // implicit solvation: -1 none, 0 ALPB, 1 GBSA
     std::string solvent;  // its solvent (xtb's names and aliases)
     int solv_state = 0;   // reference state: 0 gsolv, 1 bar1M, 2 reference
+    int dispersion = 1;   // 0: leave the D4 term out (crates/axtb/src/lib.rs:107, 185-187)
 };
 
 // ------------------------------------------------------------------ solvation parameters
@@ -301,6 +302,7 @@ size_t padded(size_t n) {
 }  // namespace
 
 // ------------------------------------------------------------------ the batch engine
+struct Moments;  // a molecule's SCC moments (capi.cuh)
 struct AxtbBatch {
     int device = 0;
     cudaStream_t st = nullptr;
@@ -311,6 +313,7 @@ struct AxtbBatch {
     int hist_cap = 0, nsp = 0;
     int mixer_kind = 0;      // the mixer plan of the run: 0 auto, 1 Broyden, 2 DIIS
     bool restart = false;    // molecules start from their previous converged moments
+    bool retry_fresh = true; // ... and one that then ends unconverged runs once more from the guess
     bool eeq_guess = true;   // the conventions start from EEQ charges
     axg::Batch B{};
     axg::State S{};
@@ -329,7 +332,10 @@ struct AxtbBatch {
     std::string err;
 
     void build(const vector<HostMol>& in, const Opt& o);
-    void run(bool want_grad, bool warm = false);
+    // want_levels: every orbital energy of the result (the SCF itself needs the lowest ones only)
+    void run(bool want_grad, bool warm = false, bool want_levels = false);
+    cudaEvent_t phase_ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, SCF start, SCF end, end
+    vector<int> h_warm;     // per molecule: the last run's result started from previous or given moments
     // profiling and traffic accounting
     struct Rec {
         const char* name;
@@ -354,10 +360,14 @@ struct AxtbBatch {
     void resolve_profile();
     void extract(AxtbResult* outs, int32_t* status, bool want_grad);
     void upload_positions(const double* host_xyz, bool device_ptr);
+    void put_moments(int m, const Moments& w);
+    Moments get_moments(int m);
     ~AxtbBatch();
 };
 
 AxtbBatch::~AxtbBatch() {
+    for (auto& e : phase_ev)
+        if (e) cudaEventDestroy(e);
     if (h_act) cudaFreeHost(h_act);
     if (h_stage) cudaFreeHost(h_stage);
     if (dmem) cudaFree(dmem);
@@ -380,6 +390,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     device = o.device;
     CK(cudaSetDevice(device));
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& e : phase_ev) CK(cudaEventCreate(&e));
     // ---- host layout
     vector<int> m_nat(nmol), m_nsh(nmol), m_nao(nmol), m_dim(nmol);
     vector<long long> m_hist0(nmol), m_pd0(nmol), m_tile0(nmol), m_wk0(nmol), m_sq0(nmol);
@@ -624,7 +635,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addD(natT * 3 + natT * 6 + nshT * 2);
     addD((size_t)nnT * 22);
     bytes += padded<unsigned char>((size_t)nnT);
-    addD((size_t)naoT * 5);
+    addD((size_t)naoT * 6);
+    addD((size_t)nmol * 2);  // Fermi levels
     addI(nmol * 7);
     addI(nmol);
     addI(nmol);
@@ -843,6 +855,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.pconv = 2e-5 * o.acc;
     b.max_iter = o.max_iter;
     b.split = o.precision == 1 ? 1 : 0;
+    b.disp = o.dispersion ? 1 : 0;
     // state
     axg::State& s = S;
     s.xyz = ar.take<double>(natT * 3);
@@ -870,6 +883,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     s.piv = ar.take<unsigned char>(nnT);
     s.emo = ar.take<double>(naoT);
     s.focc = ar.take<double>(naoT);
+    s.focc_a = ar.take<double>(naoT);
+    s.efermi = ar.take<double>((size_t)nmol * 2);
     s.dtri = ar.take<double>(naoT);
     s.etri = ar.take<double>(naoT);
     s.tau = ar.take<double>(naoT);
@@ -1158,9 +1173,11 @@ void AxtbBatch::resolve_profile() {
     recs.clear();
 }
 
-void AxtbBatch::run(bool want_grad, bool warm) {
+void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     using namespace axg;
     launches = 0;
+    h_warm.assign(nmol, warm ? 1 : 0);
+    CK(cudaEventRecord(phase_ev[0], st));
     P.cycles = profiling ? 1 : 0;
     if (profiling) {
         unsigned long long z[16] = {0};
@@ -1186,7 +1203,10 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         for (int m = 0; m < nmol; m++)
             if (act[m]) {
                 double n = mols[m].nao, k = std::ceil(mols[m].nalpha);
-                s += 4.0 * n * n * n + 4.0 / 3.0 * n * n * n + 6.0 * n * n * k;
+                // algorithmic count: n^3 (reduction to standard form, sygst), 4/3 n^3
+                // (tridiagonalisation), 2 n^2 k (Householder back-transform), n^2 k (L^-T) and
+                // n^2 k (P); the work the kernel does beyond this is overhead, not counted
+                s += n * n * n + 4.0 / 3.0 * n * n * n + 4.0 * n * n * k;
             }
         return s;
     };
@@ -1212,12 +1232,16 @@ void AxtbBatch::run(bool want_grad, bool warm) {
     LAUNCH("repulsion", 0, 0, k_repulsion<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
     LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, S.e_fixed));
     CK(cudaMemsetAsync(S.e_atom, 0, sizeof(double) * natT, st));
-    // D4 three-body at q = 0 with dgw/dCN weights
-    CK(cudaMemsetAsync(P.eeq_q, 0, sizeof(double) * natT, st));
-    LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1));
-    LAUNCH("atm_tables", 0, 0, k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT));
-    LAUNCH("atm", 0, 0, k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0));
-    LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm));
+    // D4 three-body at q = 0 with dgw/dCN weights (none without the D4 term)
+    if (B.disp) {
+        CK(cudaMemsetAsync(P.eeq_q, 0, sizeof(double) * natT, st));
+        LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1));
+        LAUNCH("atm_tables", 0, 0, k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT));
+        LAUNCH("atm", 0, 0, k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0));
+        LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm));
+    } else {
+        CK(cudaMemsetAsync(d_eatm, 0, sizeof(double) * nmol, st));
+    }
     // integrals
     LAUNCH("integrals", 0, mat_bytes(all, 11.0), k_integrals<<<blocks_for(npdT, 128), 128, 0, st>>>(B, S, d_pd0, npdT));
     if (B.solv) {  // solvation: Born radii, SASA neighbours and surfaces, ALPB shape descriptor
@@ -1286,13 +1310,26 @@ void AxtbBatch::run(bool want_grad, bool warm) {
             if (std::any_of(act.begin(), act.end(), [](int v) { return v != 0; })) scf_attempt(true);
         }
     };
+    CK(cudaEventRecord(phase_ev[1], st));
+    if (restart && !warm) {
+        CK(cudaMemcpyAsync(h_act, S.have_guess, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::copy(h_act, h_act + nmol, h_warm.begin());
+    }
     scf_plan();
     if (restart && !warm) {
         // warm starts that did not converge: the whole plan once more from the fresh guess
-        LAUNCH("fresh_mask", 0, 0, k_fresh_mask<<<blocks_for(nmol, T), T, 0, st>>>(B, S));
-        CK(cudaMemcpyAsync(h_act, S.retry, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        if (std::any_of(h_act, h_act + nmol, [](int v) { return v != 0; })) {
+        // (not for the displaced points of a numerical Hessian, which report the failure)
+        bool again = false;
+        if (retry_fresh) {
+            LAUNCH("fresh_mask", 0, 0, k_fresh_mask<<<blocks_for(nmol, T), T, 0, st>>>(B, S));
+            CK(cudaMemcpyAsync(h_act, S.retry, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            again = std::any_of(h_act, h_act + nmol, [](int v) { return v != 0; });
+        }
+        if (again) {
+            for (int m = 0; m < nmol; m++)
+                if (h_act[m]) h_warm[m] = 0;
             LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind, S.retry));
             CK(cudaMemcpyAsync(h_act, S.active, sizeof(int) * nmol, cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
@@ -1302,6 +1339,11 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         // the converged moments are the next run's starts
         CK(cudaMemcpyAsync(S.have_guess, S.conv, sizeof(int) * nmol, cudaMemcpyDeviceToDevice, st));
     }
+    if (want_levels) {
+        ph = PH_LEVELS;
+        LAUNCH("team_levels", 0, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+    }
+    CK(cudaEventRecord(phase_ev[2], st));
     if (want_grad) {
         ph = PH_WDENS;
         LAUNCH("team_wdens", w_flops(all), 0,
@@ -1325,6 +1367,7 @@ void AxtbBatch::run(bool want_grad, bool warm) {
         LAUNCH("cn_chain", 0, 0, k_cn_chain<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
     }
 #undef LAUNCH
+    CK(cudaEventRecord(phase_ev[3], st));
     CK(cudaGetLastError());
     resolve_profile();
 }

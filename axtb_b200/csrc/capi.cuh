@@ -38,10 +38,27 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     CK(cudaMemcpyAsync(qp.data(), S.qp_out, sizeof(double) * natT * 6, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(qsh.data(), S.qsh_out, sizeof(double) * nshT, cudaMemcpyDeviceToHost, st));
     if (want_grad) CK(cudaMemcpyAsync(grad.data(), S.grad, sizeof(double) * natT * 3, cudaMemcpyDeviceToHost, st));
+    // the electronic structure, when a result asks for it
+    bool levels = std::any_of(outs, outs + nmol, [](const AxtbResult& r) { return r.emo || r.focc || r.focc_alpha; });
+    vector<double> emo, focc, focca, ef(2 * (size_t)nmol);
+    if (levels) {
+        emo.resize(naoT);
+        focc.resize(naoT);
+        focca.resize(naoT);
+        CK(cudaMemcpyAsync(emo.data(), S.emo, sizeof(double) * naoT, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(focc.data(), S.focc, sizeof(double) * naoT, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(focca.data(), S.focc_a, sizeof(double) * naoT, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaMemcpyAsync(ef.data(), S.efermi, sizeof(double) * 2 * nmol, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    d2h_bytes += (long long)(sizeof(double) * (nmol * (B.solv ? 15 : 14) + (size_t)natT * 10 + nshT) +
+    d2h_bytes += (long long)(sizeof(double) * (nmol * (B.solv ? 17 : 16) + (size_t)natT * 10 + nshT) +
                              sizeof(int) * nmol * 5) +
-                 (want_grad ? (long long)sizeof(double) * natT * 3 : 0);
+                 (want_grad ? (long long)sizeof(double) * natT * 3 : 0) +
+                 (levels ? (long long)sizeof(double) * naoT * 3 : 0);
+    // phase times of this pass (events recorded by run on the stream)
+    float ms[3] = {0.0f, 0.0f, 0.0f}, tot = 0.0f;
+    for (int k = 0; k < 3; k++) CK(cudaEventElapsedTime(&ms[k], phase_ev[k], phase_ev[k + 1]));
+    CK(cudaEventElapsedTime(&tot, phase_ev[0], phase_ev[3]));
     for (int m = 0; m < nmol; m++) {
         AxtbResult& r = outs[m];
         int a0 = m_at0[m], nat = mols[m].nat;
@@ -59,6 +76,20 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
         r.residual = res[m];
         r.status = status_code(st_[m], conv[m]);
         if (status) status[m] = r.status;
+        r.nao = mols[m].nao;
+        r.fermi_levels[0] = ef[2 * (size_t)m];
+        r.fermi_levels[1] = ef[2 * (size_t)m + 1];
+        r.electronic_temperature = B.kt > 0.0 ? opt.etemp : 0.0;
+        r.warm_start = m < (int)h_warm.size() ? h_warm[m] : 0;
+        r.fallback_iterations = used[m] == 2 ? nit0[m] : 0;
+        for (int k = 0; k < 3; k++) r.timings[k] = ms[k] * 1e-3;
+        r.timings[3] = tot * 1e-3;
+        if (levels) {
+            size_t o0 = m_ao0[m], n = mols[m].nao;
+            if (r.emo) std::memcpy(r.emo, emo.data() + o0, sizeof(double) * n);
+            if (r.focc) std::memcpy(r.focc, focc.data() + o0, sizeof(double) * n);
+            if (r.focc_alpha) std::memcpy(r.focc_alpha, focca.data() + o0, sizeof(double) * n);
+        }
         if (want_grad && r.gradient)
             std::memcpy(r.gradient, grad.data() + (size_t)a0 * 3, sizeof(double) * nat * 3);
         if (r.charges) std::memcpy(r.charges, qat.data() + a0, sizeof(double) * nat);
@@ -75,11 +106,67 @@ void AxtbBatch::extract(AxtbResult* outs, int32_t* status, bool want_grad) {
     }
 }
 
+// A molecule's SCC moments (ScfGuess, crates/axtb/src/xtb.rs:204-215): shell charges (nsh),
+// atomic dipoles (nat*3) and atomic quadrupoles (nat*6).
+struct Moments {
+    vector<double> qsh, dp, qp;
+};
+
+// the moments of molecule m into the device buffers a warm start reads (the output moments of
+// the previous run; atomic charges summed from the shells)
+void AxtbBatch::put_moments(int m, const Moments& w) {
+    int a0 = m_at0[m], s0 = m_sh0[m], nat = mols[m].nat;
+    vector<double> qat(nat, 0.0);
+    for (int i = 0, s = 0; i < nat; i++)
+        for (int k = 0; k < gfn2tab::NSHELL[mols[m].Z[i] - 1]; k++, s++) qat[i] += w.qsh[s];
+    CK(cudaMemcpyAsync(S.qsh_out + s0, w.qsh.data(), sizeof(double) * w.qsh.size(), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.qat_out + a0, qat.data(), sizeof(double) * nat, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.dp_out + 3LL * a0, w.dp.data(), sizeof(double) * 3 * nat, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(S.qp_out + 6LL * a0, w.qp.data(), sizeof(double) * 6 * nat, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+}
+
+// the output moments of molecule m in the last run
+Moments AxtbBatch::get_moments(int m) {
+    Moments w;
+    int a0 = m_at0[m], s0 = m_sh0[m], nat = mols[m].nat;
+    w.qsh.resize(mols[m].nsh);
+    w.dp.resize(3 * (size_t)nat);
+    w.qp.resize(6 * (size_t)nat);
+    CK(cudaMemcpyAsync(w.qsh.data(), S.qsh_out + s0, sizeof(double) * w.qsh.size(), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(w.dp.data(), S.dp_out + 3LL * a0, sizeof(double) * 3 * nat, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(w.qp.data(), S.qp_out + 6LL * a0, sizeof(double) * 6 * nat, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return w;
+}
+
+static Moments moments_from(const HostMol& m, const double* qsh, const double* dpat, const double* qpat) {
+    if (!qsh || !dpat || !qpat) throw Fail(AXTB_ERR_INPUT, "moments: shell charges, dipoles and quadrupoles are all needed");
+    Moments w;
+    w.qsh.assign(qsh, qsh + m.nsh);
+    w.dp.assign(dpat, dpat + 3 * (size_t)m.nat);
+    w.qp.assign(qpat, qpat + 6 * (size_t)m.nat);
+    for (const auto* v : {&w.qsh, &w.dp, &w.qp})
+        for (double x : *v)
+            if (!std::isfinite(x)) throw Fail(AXTB_ERR_INPUT, "moments: non-finite value");
+    return w;
+}
+
+static void moments_to(const Moments& w, double* qsh, double* dpat, double* qpat) {
+    if (qsh) std::memcpy(qsh, w.qsh.data(), sizeof(double) * w.qsh.size());
+    if (dpat) std::memcpy(dpat, w.dp.data(), sizeof(double) * w.dp.size());
+    if (qpat) std::memcpy(qpat, w.qp.data(), sizeof(double) * w.qp.size());
+}
+
+// The calculator of one molecule (axtb::Calculator): its options, the molecule, the device
+// batch (made at the first single point) and the moments the next SCF starts from (`start`,
+// crates/axtb/src/calculator.rs:185-206; `given` when they were set from outside).
 struct AxtbHandle {
     HostMol mol;
     Opt opt;
     AxtbBatch* batch = nullptr;
-    bool have_guess = false;
+    bool have_start = false, given = false;
+    Moments start;
     std::string err;
     ~AxtbHandle() { delete batch; }
 };
@@ -99,6 +186,7 @@ static Opt to_opt(const AxtbOptions* o) {
         r.solv = o->solvation;
         r.solvent = o->solvent ? o->solvent : "";
         r.solv_state = o->solvation_state;
+        r.dispersion = o->dispersion != 0 ? 1 : 0;
     }
     return r;
 }
@@ -147,6 +235,7 @@ void axtb_gpu_default_options(AxtbOptions* o) {
     o->solvation = -1;
     o->solvent = nullptr;
     o->solvation_state = 0;
+    o->dispersion = 1;
 }
 
 int axtb_gpu_basis_size(const int32_t* numbers, int32_t nat, int32_t* nsh, int32_t* nao) {
@@ -203,17 +292,23 @@ int axtb_gpu_singlepoint(AxtbHandle* h, const double* positions, int32_t want_gr
         b.mols[0].xyz = m.xyz;
         b.upload_positions(m.xyz.data(), false);
         int32_t st = 0;
-        // warm start from the previous geometry's moments, then once more from the guess when
-        // that did not converge (crates/axtb/src/calculator.rs:194-206; the ladder climbs on
-        // ScfNotConverged only, crates/base/src/method/retry.rs:119-158)
-        bool warm = h->have_guess;
-        b.run(want_gradient != 0, warm);
+        // warm start from the previous geometry's (or the given) moments, then once more from
+        // the guess when that did not converge (crates/axtb/src/calculator.rs:194-206; the
+        // ladder climbs on ScfNotConverged only, crates/base/src/method/retry.rs:119-158)
+        bool warm = h->have_start;
+        bool lv = out->emo || out->focc || out->focc_alpha;
+        if (warm) b.put_moments(0, h->start);
+        h->have_start = h->given = false;
+        b.run(want_gradient != 0, warm, lv);
         b.extract(out, &st, want_gradient != 0);
         if (st == AXTB_ERR_SCF_NOT_CONVERGED && warm) {
-            b.run(want_gradient != 0, false);
+            b.run(want_gradient != 0, false, lv);
             b.extract(out, &st, want_gradient != 0);
         }
-        h->have_guess = st == AXTB_OK;
+        if (st == AXTB_OK) {
+            h->start = b.get_moments(0);
+            h->have_start = true;
+        }
         if (st != AXTB_OK) {
             char msg[160];
             std::snprintf(msg, sizeof msg, "SCF failed: status %d after %d iterations (dE %.3e, residual %.3e)", st,
@@ -233,6 +328,29 @@ int axtb_gpu_last_error(const AxtbHandle* h, char* buf, size_t len) {
         buf[n] = 0;
     }
     return (int)s.size();
+}
+
+int axtb_gpu_get_moments(const AxtbHandle* h, double* qsh, double* dpat, double* qpat) {
+    if (!h) return AXTB_ERR_INPUT;
+    if (!h->have_start) {
+        g_last_error = "the calculator has no moments (no converged single point and none given)";
+        return AXTB_ERR_INPUT;
+    }
+    moments_to(h->start, qsh, dpat, qpat);
+    return AXTB_OK;
+}
+
+int axtb_gpu_set_moments(AxtbHandle* h, const double* qsh, const double* dpat, const double* qpat, int32_t given) {
+    if (!h) return AXTB_ERR_INPUT;
+    return guarded(&h->err, [&] {
+        if (!qsh) {  // set_history(None): forget the moments
+            h->have_start = h->given = false;
+            return;
+        }
+        h->start = moments_from(h->mol, qsh, dpat, qpat);
+        h->have_start = true;
+        h->given = given != 0;
+    });
 }
 
 int axtb_gpu_batch_create(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, AxtbBatch** out) {
@@ -276,7 +394,8 @@ int axtb_gpu_batch_run(AxtbBatch* b, const double* positions, int32_t want_gradi
             for (auto& m : b->mols) all.insert(all.end(), m.xyz.begin(), m.xyz.end());
             b->upload_positions(all.data(), false);
         }
-        b->run(want_gradient != 0);
+        bool lv = std::any_of(outs, outs + b->nmol, [](const AxtbResult& r) { return r.emo || r.focc || r.focc_alpha; });
+        b->run(want_gradient != 0, false, lv);
         b->extract(outs, status, want_gradient != 0);
     });
 }
@@ -322,11 +441,34 @@ int axtb_gpu_batch(const AxtbMol* mols, int32_t nmol, const AxtbOptions* opts, i
 
 // ---- introspection (include/axtb_gpu_debug.h)
 int axtb_gpu_batch_set_restart(AxtbBatch* b, int32_t enable) {
-    if (!b) return AXTB_ERR_INPUT;
+    if (!b || enable < 0 || enable > 2) return AXTB_ERR_INPUT;
     return guarded(&b->err, [&] {
         b->restart = enable != 0;
+        b->retry_fresh = enable != 2;
         CK(cudaMemsetAsync(b->S.have_guess, 0, sizeof(int) * b->nmol, b->st));
         CK(cudaStreamSynchronize(b->st));
+    });
+}
+
+int axtb_gpu_batch_get_moments(AxtbBatch* b, int32_t mol, double* qsh, double* dpat, double* qpat) {
+    if (!b || mol < 0 || mol >= b->nmol) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        int conv = 0;
+        CK(cudaMemcpyAsync(&conv, b->S.conv + mol, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+        CK(cudaStreamSynchronize(b->st));
+        if (!conv) throw Fail(AXTB_ERR_INPUT, "molecule " + std::to_string(mol) + " has no converged moments");
+        moments_to(b->get_moments(mol), qsh, dpat, qpat);
+    });
+}
+
+int axtb_gpu_batch_set_moments(AxtbBatch* b, int32_t mol, const double* qsh, const double* dpat, const double* qpat) {
+    if (!b || mol < 0 || mol >= b->nmol) return AXTB_ERR_INPUT;
+    return guarded(&b->err, [&] {
+        b->put_moments(mol, moments_from(b->mols[mol], qsh, dpat, qpat));
+        int one = 1;
+        CK(cudaMemcpyAsync(b->S.have_guess + mol, &one, sizeof(int), cudaMemcpyHostToDevice, b->st));
+        CK(cudaStreamSynchronize(b->st));
+        b->restart = true;
     });
 }
 

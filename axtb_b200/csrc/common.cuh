@@ -80,6 +80,7 @@ struct Batch {
     const double *sv_vdwr, *sv_rho, *sv_svdw, *sv_vdwsa, *sv_t1, *sv_t2, *sv_wrp, *sv_gam, *sv_hbmag;
     const double* sv_srcut;
     int split;                        // 1: basis-transform and W GEMMs in split precision
+    int disp;                         // 0: the D4 term is left out (Options::dispersion = false)
 };
 
 // per-geometry and per-iteration device state
@@ -94,6 +95,8 @@ struct State {
     double *scr1, *scr2, *scr3;  // nnT each: inverse-iteration / back-transform scratch
     unsigned char* piv;          // nnT
     double *emo, *focc;          // naoT
+    double* focc_a;              // naoT: alpha occupations (NULL: not kept)
+    double* efermi;              // 2 nmol: alpha and beta Fermi levels (NaN: aufbau filling; NULL: not kept)
     double *dtri, *etri, *tau;   // naoT: tridiagonal and Householder factors
     int* kocc;                   // nmol
     // SCC moments (input = mixed, output = Mulliken)

@@ -221,7 +221,7 @@ __device__ __forceinline__ void pair_c6(const Batch& B, const State& S, int a, i
 // two-body damped pair factor with its smooth switch (crates/d4/src/disp.rs:298-322):
 // pe (energy factor), pg (radial derivative / r); false outside the cutoff
 __device__ __forceinline__ bool d4_pair(const Batch& B, int spa, int spb, double r2, double& pe, double& pg) {
-    if (r2 > B.d2_cut * B.d2_cut || r2 < DBL_EPSILON) return false;
+    if (!B.disp || r2 > B.d2_cut * B.d2_cut || r2 < DBL_EPSILON) return false;
     double r = sqrt(r2), sw, dsw;
     smooth_cut(r, B.d2_cut, B.d2_w, sw, dsw);
     if (sw <= 0.0) return false;

@@ -7,13 +7,15 @@
 //   PH_EIGEN    F' = L^-1 F L^-T, eigenvalues, tblite Fermi filling, occupied eigenvectors,
 //               C = L^-T Q Z and P = C f C^T (crates/axtb/src/xtb.rs:997-1038)
 //   PH_WDENS    W = C (f e) C^T (crates/axtb/src/xtb.rs:688-696)
+//   PH_LEVELS   the orbital energies above the ones the SCF needed, from the last tridiagonal
+//               matrix (all levels, as the reference's eigensolver returns them for the result)
 #pragma once
 #include "common.cuh"
 #include "team_la.cuh"
 
 namespace axg {
 
-enum { PH_OVERLAP = 0, PH_EEQ = 1, PH_EIGEN = 2, PH_WDENS = 3 };
+enum { PH_OVERLAP = 0, PH_EEQ = 1, PH_EIGEN = 2, PH_WDENS = 3, PH_LEVELS = 4 };
 
 struct TeamPlan {
     const int* big;        // molecules run by the whole grid
@@ -100,8 +102,10 @@ __device__ void mol_fermi(const Team& t, const Batch& B, State& S, int m, const 
         int lane = threadIdx.x;
         double pa = 0.0, pb = 0.0, ts = 0.0, flast = 0.0;
         int kl = 0;
+        double* falpha = S.focc_a ? S.focc_a + B.m_ao0[m] : nullptr;
         for (int i = lane; i < n; i += 32) {
             double fa = focc[i], fb = occb[i];
+            if (falpha) falpha[i] = fa;
             pa += fa;
             pb += fb;
             if (B.kt > 0.0) ts += log(pow(fa, fa) * pow(1.0 - fa, 1.0 - fa)) + log(pow(fb, fb) * pow(1.0 - fb, 1.0 - fb));
@@ -120,6 +124,11 @@ __device__ void mol_fermi(const Team& t, const Batch& B, State& S, int m, const 
         if (lane == 0) {
             S.kocc[m] = kl;
             S.ts[m] = ts * B.kt;
+            if (S.efermi) {  // the Fermi levels, NaN where the filling is aufbau (0 K, no electrons)
+                bool fa = B.kt > 0.0 && B.m_nalpha[m] > 0.0, fb = B.kt > 0.0 && B.m_nbeta[m] > 0.0;
+                S.efermi[2 * m] = fa ? efa : __longlong_as_double(0x7ff8000000000000LL);
+                S.efermi[2 * m + 1] = fb ? efb : __longlong_as_double(0x7ff8000000000000LL);
+            }
             *more = (kc < n && flast > 1e-16) ? 1.0 : 0.0;
             if (fabs(pa - B.m_nalpha[m]) > 1e-6 || fabs(pb - B.m_nbeta[m]) > 1e-6) atomicOr(&S.status[m], ST_FERMI);
         }
@@ -224,6 +233,20 @@ __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPla
     t.sync();
 }
 
+// Every orbital energy of the last eigen phase: the SCF bisects only the lowest
+// ceil(n_occ) + max(16, n/16) levels of the tridiagonal matrix (or all of them), the rest
+// holding the Gershgorin bound; this bisects the rest of the same (d, e).
+__device__ void mol_levels(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+    int n = B.m_nao[m], ao0 = B.m_ao0[m];
+    double* wk = P.wk + P.m_wk0[m];
+    const double* d = S.dtri + ao0;
+    const double* e = S.etri + ao0;
+    int kc = min(n, (int)ceil(fmax(B.m_nalpha[m], B.m_nbeta[m])) + max(16, n / 16));
+    if (kc >= n) return;
+    team_gershgorin(t, d, e, n, wk);
+    team_bisect(t, d, e, n, S.emo + ao0, wk, kc, n);
+}
+
 __device__ __forceinline__ bool phase_wants(const State& S, int phase, int m) {
     if (phase == PH_EIGEN) return S.active[m] != 0;
     if (phase == PH_WDENS) return S.conv[m] != 0;
@@ -236,6 +259,7 @@ __device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan&
         case PH_EEQ: mol_eeq(t, B, S, P, m); break;
         case PH_EIGEN: mol_eigen(t, B, S, P, m); break;
         case PH_WDENS: mol_wdens(t, B, S, P, m); break;
+        case PH_LEVELS: mol_levels(t, B, S, P, m); break;
     }
 }
 

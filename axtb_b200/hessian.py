@@ -1,14 +1,16 @@
-"""Semi-numerical Hessian from central differences of analytic gradients, all displacements in
-one batch on the GPU.
+"""Semi-numerical Hessian from central differences of analytic gradients, the displacements in
+batches on the GPU.
 
 axtb's numerical Hessian (``Calculator::numerical_hessian``, crates/axtb/src/calculator.rs:266-296,
-with crates/base/src/fd.rs:39-41, 122-140, 170-207): a reference single point, then every
+with crates/base/src/fd.rs:39-41, 122-140, 170-207): one reference single point, then every
 Cartesian coordinate moved forward by the step and back by twice the step, every displaced SCF
-converged to min(accuracy, 0.01) starting from the reference's converged moments; row y of the
-matrix holds the central difference of the gradients along coordinate y (its column y, the same
-once symmetrized), the matrix is replaced by its symmetric part (the largest asymmetry is
-reported), and the dipole derivatives come from the same points. Here the 6N displaced single
-points are one ``Batch`` run, each molecule restarting from the reference's moments.
+converged to min(accuracy, 0.01) starting from the reference's converged moments (a displaced
+SCF that does not converge from them is an error, with no second run from the guess); row y of
+the matrix holds the central difference of the gradients along coordinate y (its column y, the
+same once symmetrized), the matrix is replaced by its symmetric part (the largest asymmetry is
+reported), and the dipole derivatives come from the same points. Here the reference is one
+single point and the 6N displaced single points run as ``Batch`` runs of as many copies as fit
+the free device memory, each copy seeded with the reference's moments.
 """
 from __future__ import annotations
 
@@ -16,7 +18,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .calculator import AxtbError, Batch, SinglePoint
+from .calculator import AxtbError, Batch, SinglePoint, basis_size
 
 NUMERICAL_ACCURACY = 0.01  # crates/axtb/src/calculator.rs:86
 
@@ -62,31 +64,59 @@ def assemble(gplus, gminus, dplus, dminus, step: float):
     return h, dipd, asym
 
 
-def numerical_hessian(numbers, positions, charge=0.0, uhf=None, step=0.005, accuracy=None, **options) -> Hessian:
+def copies_that_fit(nao: int, ncopies: int, device: int = 0) -> int:
+    """How many copies of an nao-AO molecule one batch may hold: the engine keeps about 23 dense
+    nao x nao FP64 planes per molecule, and a batch gets at most half of the free device memory."""
+    per = 8.0 * 23.0 * max(nao, 64) ** 2 + 1.0e6
+    try:
+        import torch
+
+        free = torch.cuda.mem_get_info(device)[0]
+    except Exception:
+        free = 16.0e9
+    return max(1, min(ncopies, int(0.5 * free / per)))
+
+
+def numerical_hessian(numbers, positions, charge=0.0, uhf=None, step=0.005, accuracy=None, max_batch=None,
+                      **options) -> Hessian:
     """Semi-numerical Hessian of one molecule (positions in bohr; step in bohr, 0.005 axtb's
-    suggestion). ``accuracy``: the SCF accuracy of the displaced points (default 0.01, never
-    looser than the options' own accuracy); the other options as for ``Calculator``."""
+    suggestion). ``accuracy``: the SCF accuracy of the reference and displaced points (default
+    0.01, never looser than the options' own accuracy); ``max_batch``: most displaced copies per
+    batch (default: as many as fit half of the free device memory); the other options as for
+    ``Calculator``."""
     if not (step > 0.0 and np.isfinite(step)):
         raise AxtbError(1, f"the Hessian step must be a positive number, got {step}")
     x0 = np.asarray(positions, dtype=np.float64).reshape(-1, 3)
     acc = min(NUMERICAL_ACCURACY if accuracy is None else float(accuracy), float(options.pop("accuracy", 1.0)))
-    pts = displacements(x0, step)
     z = np.asarray(numbers, dtype=np.int32)
-    batch = Batch([(z, x0, charge, uhf)] * (1 + len(pts)), accuracy=acc, **options)
+    # the reference single point, once; its converged moments start every displaced SCF
+    ref = Batch([(z, x0, charge, uhf)], accuracy=acc, **options)
     try:
-        batch.set_restart(True)
-        first = batch.run(gradient=True)  # the reference single point (every copy holds its moments)
-        if first[0].status != 0:
-            raise AxtbError(first[0].status, "the reference single point of the Hessian failed")
-        res = batch.run(positions=[x0] + pts, gradient=True)
-        bad = [i for i, r in enumerate(res[1:]) if r.status != 0]
-        if bad:
-            raise AxtbError(res[1 + bad[0]].status, f"{len(bad)} displaced single points of the Hessian failed")
-        gp = [r.gradient for r in res[1::2]]
-        gm = [r.gradient for r in res[2::2]]
-        dp = [r.dipole for r in res[1::2]]
-        dm = [r.dipole for r in res[2::2]]
-        h, dipd, asym = assemble(gp, gm, dp, dm, step)
-        return Hessian(hessian=h, dipole_derivatives=dipd, max_asymmetry=asym, reference=first[0])
+        first = ref.run(gradient=True)[0]
+        if first.status != 0:
+            raise AxtbError(first.status, "the reference single point of the Hessian failed")
+        start = ref.get_moments(0)
     finally:
-        batch.close()
+        ref.close()
+    pts = displacements(x0, step)
+    chunk = int(max_batch) if max_batch else copies_that_fit(basis_size(z)[1], len(pts), options.get("device", 0))
+    res = []
+    for c0 in range(0, len(pts), chunk):
+        part = pts[c0:c0 + chunk]
+        batch = Batch([(z, p, charge, uhf) for p in part], accuracy=acc, **options)
+        try:
+            batch.set_restart(True, retry_fresh=False)
+            for i in range(len(part)):
+                batch.set_moments(i, start)
+            res += batch.run(gradient=True)
+        finally:
+            batch.close()
+    bad = [i for i, r in enumerate(res) if r.status != 0]
+    if bad:
+        raise AxtbError(res[bad[0]].status, f"{len(bad)} displaced single points of the Hessian failed")
+    gp = [r.gradient for r in res[0::2]]
+    gm = [r.gradient for r in res[1::2]]
+    dp = [r.dipole for r in res[0::2]]
+    dm = [r.dipole for r in res[1::2]]
+    h, dipd, asym = assemble(gp, gm, dp, dm, step)
+    return Hessian(hessian=h, dipole_derivatives=dipd, max_asymmetry=asym, reference=first)

@@ -73,6 +73,8 @@ typedef struct AxtbOptions {
                           axtb_gpu_create / axtb_gpu_batch_create only */
     int32_t solvation_state; /* reference state of the solvation free energy: 0 gsolv (default),
                           1 bar1M, 2 reference */
+    int32_t dispersion;  /* 1 (default): with the D4 dispersion term; 0: without it (Options::dispersion,
+                          crates/axtb/src/lib.rs:106-107, 185-187: for validation only) */
 } AxtbOptions;
 
 /* Results of one single point (crates/base/src/method/results.rs:39-57). Array members are
@@ -96,6 +98,21 @@ typedef struct AxtbResult {
                                2 DIIS after Broyden did not converge ("diis-fallback") */
     double solvation;       /* the solvation term (surface, shift and polar parts; part of the
                                electronic subtotal as in crates/axtb/src/calculator.rs:301-316); 0 without */
+    /* the electronic structure (Electronic of crates/base/src/method/results.rs:77-142) */
+    double* emo;            /* nao orbital energies (Eh), ascending: every level (OrbitalLevels::energies) */
+    double* focc;           /* nao occupations of both spins together (0..2) */
+    double* focc_alpha;     /* nao alpha occupations (beta = focc - focc_alpha) */
+    double fermi_levels[2]; /* alpha and beta Fermi levels (Eh); NaN where the occupations are the
+                               aufbau filling (0 K, or no electrons of that spin) */
+    double electronic_temperature; /* K of the occupations; 0 where they are the aufbau filling */
+    int32_t nao;            /* basis functions: the length of emo, focc, focc_alpha */
+    int32_t warm_start;     /* 1: the SCF of the result started from previous or given moments
+                               (ScfReport::start "previous"), 0: from the guess */
+    int32_t fallback_iterations; /* iterations of the Broyden attempt that the DIIS fallback replaced
+                               (mixer_used 2; ScfReport::attempts), 0 otherwise */
+    double timings[4];      /* wall time (s) of the device pass the result came from: set-up
+                               (geometry, integrals, overlap factorisation, guess), scf, gradient,
+                               total (SinglePoint::timings; a batch reports the batch's pass) */
 } AxtbResult;
 
 /* One molecule of a batch: atomic numbers, positions (bohr, nat*3 row-major), charge and the
@@ -126,6 +143,21 @@ int axtb_gpu_create(const int32_t* numbers, int32_t nat, double charge, int32_t 
  * that start fails (crates/axtb/src/calculator.rs:194-206). */
 int axtb_gpu_singlepoint(AxtbHandle* h, const double* positions, int32_t want_gradient, AxtbResult* out);
 
+/* The SCC moments the calculator's next SCF starts from: shell charges (nsh), atomic dipoles
+ * (nat*3) and atomic quadrupoles (nat*6, xx, xy, yy, xz, yz, zz) -- the converged moments of its
+ * last successful single point, or the ones given to it (Method::wavefunction,
+ * crates/axtb/src/calculator.rs:413-423). Any output may be NULL. AXTB_ERR_INPUT when it has none
+ * (before the first converged single point, or after a failed one: reset_wavefunction). */
+int axtb_gpu_get_moments(const AxtbHandle* h, double* qsh, double* dpat, double* qpat);
+
+/* Start the next SCF from these moments (sizes as above; another calculator's or another
+ * program's converged moments): given = 1 is Method::set_wavefunction, given = 0 is
+ * Method::set_history(Some) (crates/axtb/src/calculator.rs:425-442; this calculator always reuses
+ * previous moments, so the two start the same way). qsh = NULL forgets them
+ * (set_history(None)). The single point that starts from them still runs once more from the
+ * guess when it does not converge. */
+int axtb_gpu_set_moments(AxtbHandle* h, const double* qsh, const double* dpat, const double* qpat, int32_t given);
+
 void axtb_gpu_destroy(AxtbHandle* h);
 
 /* Message of the last failed call on `h` (or of the last failed handle-less call when h is
@@ -152,8 +184,18 @@ int axtb_gpu_batch_run_device(AxtbBatch* b, const double* d_positions, int32_t w
  * each molecule from its converged moments of the previous run (a molecule without them from
  * the guess), and a molecule that then ends unconverged runs once more from the guess, as each
  * molecule's axtb::Calculator does under Restart::Previous (crates/axtb/src/calculator.rs:185-206,
- * crates/base/src/method/retry.rs:150-158). enable = 0 (the default) forgets the moments. */
+ * crates/base/src/method/retry.rs:150-158). enable = 2 is the same without the second run from
+ * the guess: a molecule whose warm start does not converge reports the failure, as the displaced
+ * points of axtb's numerical Hessian do (crates/axtb/src/calculator.rs:273-284). enable = 0 (the
+ * default) forgets the moments. Every call forgets the moments of the previous run. */
 int axtb_gpu_batch_set_restart(AxtbBatch* b, int32_t enable);
+/* Molecule mol's converged output moments of the last run (sizes as for axtb_gpu_get_moments;
+ * any output may be NULL); AXTB_ERR_INPUT when it did not converge. */
+int axtb_gpu_batch_get_moments(AxtbBatch* b, int32_t mol, double* qsh, double* dpat, double* qpat);
+/* Start molecule mol of the next run from these moments (a session lineage's previous moments,
+ * or the reference point of a Hessian's displacements); turns restarts on (enable = 1 unless
+ * axtb_gpu_batch_set_restart chose 2 before). */
+int axtb_gpu_batch_set_moments(AxtbBatch* b, int32_t mol, const double* qsh, const double* dpat, const double* qpat);
 /* The CUDA stream (cudaStream_t) the batch runs on, for callers that time or order work. */
 void* axtb_gpu_batch_stream(AxtbBatch* b);
 /* Number of kernels the last run launched (counted on the host at each launch). */

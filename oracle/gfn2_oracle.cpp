@@ -971,6 +971,7 @@ struct D4 {
     vector<double> c6ref;  // [isp*nsp+jsp][7][7]
     vector<double> rr, r0;
     vector<double> cn;
+    bool off = false;  // Options::dispersion = false: the term is left out (crates/axtb/src/lib.rs:185-187)
     // two-body pair list (i > j)
     vector<int> pi, pj;
     vector<double> pe, pg;
@@ -2447,10 +2448,11 @@ int run(OracleRun* R) {
     vector<double> gam = es2_gamma(md);
     AesCache ac = aes_cache(md, cn);
     D4 d4 = d4_setup(m);
+    d4.off = R->no_dispersion != 0;
     bool wantg = R->want_gradient != 0;
     vector<double> grad(3 * nat, 0.0), dedcn(nat, 0.0);
     double e_rep = repulsion(md, wantg ? &grad : nullptr);
-    double e_atm = d4_atm(d4, m, wantg ? &grad : nullptr);
+    double e_atm = d4.off ? 0.0 : d4_atm(d4, m, wantg ? &grad : nullptr);
     // implicit solvation: geometry part, surface energy and shift (crates/axtb/src/solvation.rs:66-75)
     bool solv = R->solv_model >= 0;
     Solv sv;
@@ -2531,7 +2533,7 @@ int run(OracleRun* R) {
             }
             for (int a = 0; a < nsh; a++) pot.vsh[a] += state.qsh[a] * state.qsh[a] * md.gam3[a];
             aes_potential(md, ac, state.qat, state.dp, state.qp, pot.vat, pot.vdp, pot.vqp);
-            d4_energy(d4, state.qat, &pot.vat);
+            if (!d4.off) d4_energy(d4, state.qat, &pot.vat);
             if (solv) solv_potential(sv, state.qat, pot.vat);
             // Fock (crates/axtb/src/scf/fock.rs:22-104)
             vector<double> B((size_t)nao * nao);
@@ -2615,7 +2617,7 @@ int run(OracleRun* R) {
             double e3 = 0.0;
             for (int a = 0; a < nsh; a++) e3 += out.qsh[a] * out.qsh[a] * out.qsh[a] * md.gam3[a] / 3.0;
             double eaes = aes_energy(md, ac, out.qat, out.dp, out.qp);
-            double edisp = d4_energy(d4, out.qat, nullptr);
+            double edisp = d4.off ? 0.0 : d4_energy(d4, out.qat, nullptr);
             double band = 0.0;
             for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
             double esolv = solv ? solv_energy(sv, out.qat) : 0.0;
@@ -2699,7 +2701,7 @@ int run(OracleRun* R) {
         }
         es2_grad(md, out.qsh, grad);
         aes_grad(md, ac, out.qat, out.dp, out.qp, grad, dedcn);
-        d4_grad(d4, m, out.qat, grad);
+        if (!d4.off) d4_grad(d4, m, out.qat, grad);
         if (solv) solv_gradient(sv, m, out.qat, grad);
         // H0/S/D/Q derivative contraction (crates/axtb/src/hamiltonian.rs:101-223)
         vector<double> vao(nao);

@@ -33,6 +33,8 @@ typedef struct {
     int solv_model;          /* implicit solvation: -1 none, 0 ALPB, 1 GBSA */
     const char* solvent;     /* solvent name (xtb's names and aliases) */
     int solv_state;          /* reference state: 0 gsolv, 1 bar1M, 2 reference */
+    int no_dispersion;       /* 1: leave the D4 term out (Options::dispersion = false,
+                                crates/axtb/src/lib.rs:185-187); 0: with it (default) */
     /* outputs (caller-allocated; any may be NULL) */
     double* energy;
     double* gradient;        /* nat*3 */

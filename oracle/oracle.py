@@ -24,7 +24,7 @@ class _Run(C.Structure):
         ("charge", C.c_double), ("uhf", C.c_int), ("accuracy", C.c_double), ("etemp", C.c_double),
         ("max_iter", C.c_int), ("want_gradient", C.c_int), ("eig_backend", C.c_int),
         ("lapack_threads", C.c_int), ("mixer", C.c_int), ("conventions", C.c_int),
-        ("solv_model", C.c_int), ("solvent", C.c_char_p), ("solv_state", C.c_int),
+        ("solv_model", C.c_int), ("solvent", C.c_char_p), ("solv_state", C.c_int), ("no_dispersion", C.c_int),
         ("energy", C.POINTER(C.c_double)), ("gradient", C.POINTER(C.c_double)),
         ("qat", C.POINTER(C.c_double)), ("qsh", C.POINTER(C.c_double)),
         ("dpat", C.POINTER(C.c_double)), ("qpat", C.POINTER(C.c_double)),
@@ -49,8 +49,8 @@ TERM_NAMES = ("repulsion", "dispersion", "electronic", "isotropic_es", "third_or
 
 def build() -> Path:
     """Compile the oracle (``make -C oracle``) if its library is missing or stale."""
-    src = HERE / "gfn2_oracle.cpp"
-    if not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+    src = max((HERE / f).stat().st_mtime for f in ("gfn2_oracle.cpp", "gfn2_oracle.h", "Makefile"))
+    if not LIB.exists() or LIB.stat().st_mtime < src:
         subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
     return LIB
 
@@ -105,13 +105,13 @@ def sizes(numbers):
 
 def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=300.0, max_iter=250,
                 gradient=True, matrices=False, lapack=False, lapack_threads=1, mixer=None, failed=False,
-                conventions="axtb", solvation=None):
+                conventions="axtb", solvation=None, dispersion=True):
     """Run the oracle; returns a dict (energy, gradient, qat, qsh, dpat, qpat, dipole, terms, emo,
     focc, iterations, converged, mixer_used[, density, wdensity]). ``mixer``: None (the
     conventions' mixer: auto for axtb, Broyden for xtb and tblite), "auto" (Broyden, then DIIS
     from the start guess), "broyden" or "diis"; ``conventions``: "axtb", "xtb" (6.8.0) or
     "tblite" (0.8.0); ``solvation``: None or (model "alpb" | "gbsa", solvent, state "gsolv" |
-    "bar1M" | "reference"). Raises RuntimeError on a failed SCF
+    "bar1M" | "reference"); ``dispersion``: False leaves the D4 term out. Raises RuntimeError on a failed SCF
     unless ``failed`` (then the dict of the failed run carries ``status`` and ``error``)."""
     z = np.ascontiguousarray(numbers, dtype=np.int32)
     x = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
@@ -143,6 +143,7 @@ def singlepoint(numbers, positions, charge=0.0, uhf=None, accuracy=1.0, etemp=30
     r.solv_model = SOLV_MODELS[model]
     r.solvent = solvent.encode()
     r.solv_state = SOLV_STATES[state.lower()]
+    r.no_dispersion = 0 if dispersion else 1
     for k in ("energy", "gradient", "qat", "qsh", "dpat", "qpat", "dipole", "terms", "emo", "focc"):
         setattr(r, k, _p(out[k]))
     if matrices:

@@ -10,7 +10,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def test_reference_arm_json_line():
     out = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--nmol", "16", "--steps", "1",
-                          "--warmup", "1", "--cpu-budget", "1"], capture_output=True, text=True, timeout=300,
+                          "--warmup", "1"], capture_output=True, text=True, timeout=300,
                          check=True).stdout.strip().splitlines()
     assert len(out) == 1
     d = json.loads(out[0])
@@ -20,3 +20,4 @@ def test_reference_arm_json_line():
     assert d["impl"] == "reference" and d["unit"] == "mol/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    assert d["config"]["sample_per_step"] == 16  # the whole (tiny) batch each step

@@ -64,3 +64,56 @@ def test_unconverged_restart_runs_again_from_the_guess(engine):
     assert r.energy == cold.energy and np.array_equal(r.gradient, cold.gradient)
     assert prof["kernels"]["start"]["launches"] == 2 and prof["kernels"]["start_warm"]["launches"] == 1
     b.close()
+
+
+def test_moments_seed_another_calculator(engine):
+    """Session lineages across calculators (Method::wavefunction / set_wavefunction /
+    set_history, crates/axtb/src/calculator.rs:413-447, through axtb_gpu_get_moments and
+    axtb_gpu_set_moments): a fresh calculator seeded with another's converged moments takes the
+    same warm-started SCF as that calculator itself (same iterations, same bits), and a batch
+    molecule seeded the same way through axtb_gpu_batch_set_moments agrees with it."""
+    from axtb_b200 import structures as S
+
+    z, x = S.water_cluster(12, seed=7)
+    moved = x + np.random.default_rng(1).normal(scale=0.02, size=x.shape)
+    a = engine.Calculator(z, x, accuracy=1e-6)
+    assert a.wavefunction() is None
+    a.singlepoint(x)
+    w = a.wavefunction()
+    assert w is not None and w.qsh.size == engine.basis_size(z)[0]
+    ra = a.singlepoint(moved)  # warm start from its own moments at x
+    cold = engine.Calculator(z, x, accuracy=1e-6).singlepoint(moved)
+    assert ra.iterations < cold.iterations
+    for given in (True, False):
+        b = engine.Calculator(z, x, accuracy=1e-6)
+        (b.set_wavefunction if given else b.set_history)(w)
+        rb = b.singlepoint(moved)
+        assert rb.iterations == ra.iterations
+        assert rb.energy == ra.energy and np.array_equal(rb.gradient, ra.gradient)
+    c = engine.Calculator(z, x, accuracy=1e-6)
+    c.set_history(w)
+    c.set_history(None)  # forgotten: a cold start
+    assert c.singlepoint(moved).iterations == cold.iterations
+    batch = engine.Batch([(z, moved)], accuracy=1e-6)
+    batch.set_moments(0, w)
+    rbt = batch.run()[0]
+    assert rbt.iterations == ra.iterations and abs(rbt.energy - ra.energy) < 1e-12
+    wb = batch.get_moments(0)
+    assert np.abs(wb.qsh - rb.qsh).max() < 1e-10
+    batch.close()
+
+
+def test_dispersion_off_matches_oracle(engine, golden):
+    """Options::dispersion = false (crates/axtb/src/lib.rs:185-187) leaves the D4 term out; the
+    oracle with the same switch gives the same energy and gradient, and the dispersion term is 0."""
+    from oracle import oracle as O
+
+    c = golden["struct-caffeine"]
+    z, x = np.array(c["numbers"]), np.array(c["positions"])
+    r = engine.Calculator(z, x, accuracy=1e-6, dispersion=False).singlepoint(x)
+    ref = O.singlepoint(z, x, accuracy=1e-6, dispersion=False)
+    full = O.singlepoint(z, x, accuracy=1e-6)
+    assert r.terms["dispersion"] == 0.0 and ref["terms"]["dispersion"] == 0.0
+    assert abs(full["energy"] - ref["energy"]) > 1e-3
+    assert abs(r.energy - ref["energy"]) < 1e-9
+    assert np.abs(r.gradient - ref["gradient"]).max() < 1e-8
