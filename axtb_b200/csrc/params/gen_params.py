@@ -18,7 +18,7 @@ double arithmetic, which rounds exactly as the Rust constant evaluation does, an
 
 Run from the repository root::
 
-    python axtb_b200/csrc/params/gen_params.py [path-to-axtb-checkout]
+    python axtb_b200/csrc/params/gen_params.py <path-to-axtb-checkout>
 
 The output header is committed; the script only needs the axtb sources to regenerate it.
 """
@@ -29,7 +29,9 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path-to-axtb-checkout>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).with_name("gfn2_tables.h")
 
 EVTOAU = 1.0 / 27.21138505

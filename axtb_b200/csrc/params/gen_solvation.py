@@ -8,7 +8,7 @@ writes the parameter sets, the name tables and the default 230-point angular gri
 expanded from its Oh generators in xtb's point order (``lebedev.f90`` genOh1..genOh6), so that
 surface sums run in the reference's order. Run once in a checkout that has the axtb sources::
 
-    python axtb_b200/csrc/params/gen_solvation.py [path-to-axtb-checkout]
+    python axtb_b200/csrc/params/gen_solvation.py <path-to-axtb-checkout>
 """
 from __future__ import annotations
 
@@ -17,7 +17,9 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path-to-axtb-checkout>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).with_name("solvation_tables.h")
 SRC = REF / "crates" / "solvation" / "src"
 DEFAULT_GRID = 230

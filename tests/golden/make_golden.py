@@ -20,7 +20,7 @@ results, plus axtb's energies and iterations in its xtb (6.8.0) and tblite (0.8.
 the cases of the solvation category (ALPB or GBSA, solvent, reference state) with axtb's recorded
 energies. Run once in a checkout that has the axtb sources::
 
-    python tests/golden/make_golden.py [path-to-axtb-checkout]
+    python tests/golden/make_golden.py <path-to-axtb-checkout>
 """
 from __future__ import annotations
 
@@ -28,7 +28,9 @@ import json
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path-to-axtb-checkout>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).with_name("reference_matrix.json")
 SOLV = Path(__file__).with_name("solvation.json")
 KEEP = {"elements", "structures", "multielement", "charges", "spin", "etemp_acc", "open_shell_metals", "threads"}

@@ -15,7 +15,7 @@ does (coordinate x AATOAU of ``tests/reference_matrix/structures.py``) and write
 
 Run once in a checkout that has the axtb sources::
 
-    python tests/golden/make_scf_hard.py [path-to-axtb-checkout]
+    python tests/golden/make_scf_hard.py <path-to-axtb-checkout>
 """
 from __future__ import annotations
 
@@ -24,7 +24,9 @@ import re
 import sys
 from pathlib import Path
 
-REF = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {Path(__file__).name} <path-to-axtb-checkout>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).with_name("scf_hard.json")
 METHODS = ("axtb-broyden", "axtb-diis", "axtb-auto")
 
