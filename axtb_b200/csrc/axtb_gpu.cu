@@ -585,7 +585,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     int per = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, axg::k_team, axg::TEAM_THREADS, 0));
+    CK(cudaFuncSetAttribute((const void*)axg::k_team, cudaFuncAttributeMaxDynamicSharedMemorySize, axg::SMEM_WORK_BYTES));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, axg::k_team, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES));
     if (per <= 0) throw Fail(AXTB_ERR_DEVICE, "team kernel does not fit on a multiprocessor");
     grid = nsm * std::min(per, 2);
     vector<int> big, small_off(grid + 1, 0), small_list;
@@ -1258,7 +1259,7 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     double chol_flops = 0.0;
     for (int m = 0; m < nmol; m++) chol_flops += (1.0 / 3.0 + 2.0 / 3.0) * std::pow((double)mols[m].nao, 3.0);
     LAUNCH("team_overlap", chol_flops, 0,
-           CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+           CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
     bool eeq = opt.guess == 0 && eeq_guess && !warm;
     if (warm) {
         LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind, nullptr));
@@ -1267,7 +1268,7 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
         ph = PH_EEQ;
         double f = 0.0;
         for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
-        LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+        LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
     }
     if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind, nullptr));
     // restarts: a molecule with converged moments from the previous run starts from them
@@ -1284,7 +1285,7 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
             LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
             ph = PH_EIGEN;
             LAUNCH("team_eigen", eig_flops(act), 0,
-                   CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+                   CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
             LAUNCH("mulliken", 0, mat_bytes(act, 12.0),
                    k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S));
             LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
@@ -1341,13 +1342,13 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     }
     if (want_levels) {
         ph = PH_LEVELS;
-        LAUNCH("team_levels", 0, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+        LAUNCH("team_levels", 0, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
     }
     CK(cudaEventRecord(phase_ev[2], st));
     if (want_grad) {
         ph = PH_WDENS;
         LAUNCH("team_wdens", w_flops(all), 0,
-               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, 0, st)));
+               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
         if (B.output_aes)
             LAUNCH("gradient_potentials", 0, 0,
                    k_gradient_potentials_aes<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
@@ -1444,9 +1445,12 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
             // host code only holds a stand-in for the array: its device address comes from the
             // runtime, once per device, with that device current
             cudaError_t e = cudaGetSymbolAddress((void**)&g_static_addr[dev], g_density_scratch);
+            if (e == cudaSuccess)  // the kernel's dynamic shared work area (no device allocation)
+                e = cudaFuncSetAttribute((const void*)axg::k_density_static, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         axg::SMEM_WORK_BYTES);
             if (e != cudaSuccess) {
                 g_static_addr[dev] = nullptr;
-                g_last_error = std::string("axtb_gpu_density_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+                g_last_error = std::string("axtb_gpu_density_static: device set-up: ") + cudaGetErrorString(e);
                 return AXTB_ERR_DEVICE;
             }
         }
@@ -1492,7 +1496,8 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.P = d_density;
     B.nmol = 1;
     B.kt = kt;
-    axg::k_density_static<<<1, axg::TEAM_THREADS, 0, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta, d_status);
+    axg::k_density_static<<<1, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta,
+                                                                                              d_status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         g_last_error = std::string("axtb_gpu_density_static: launch: ") + cudaGetErrorString(e);

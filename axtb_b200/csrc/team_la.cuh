@@ -108,32 +108,49 @@ __device__ double team_sum(const Team& t, double v, double* gred) {
 // C(MxN) = alpha op(A) op(B) + beta C; op(A) = A (M x K, lda) or A^T (A is K x M);
 // op(B) = B (K x N, ldb) or B^T (B is N x K). 64x64 CTA tiles on FP64 tensor cores
 // (mma.sync m8n8k4.f64: each of the 8 warps owns a 32x16 block of 4x2 MMA tiles), k-steps of 16
-// staged through two shared-memory buffers with the next step's global loads in flight in
-// registers while the current step computes. Flags restrict the work to the non-zero part of
-// structured operands (exactly: the skipped products are zero) or of symmetric results:
+// fed through a GSTAGES-deep ring of shared-memory stages by asynchronous copies (cp.async, 8
+// bytes per element, zero-filled outside the operands), so the loads of GSTAGES - 1 k-steps are
+// in flight while one computes. Flags restrict the work to the non-zero part of structured
+// operands (exactly: the skipped products are zero) or of symmetric results:
 //   GEMM_A_LOWER  op(A) lower triangular: k <= row      GEMM_A_UPPER  op(A) upper: k >= row
 //   GEMM_B_UPPER  op(B) upper triangular: k <= col      GEMM_B_LOWER  op(B) lower: k >= col
 //   GEMM_LOWER_TILES  only tiles with bi >= bj
+//   GEMM_A_SYMM   A is symmetric (M x M) and only its lower triangle is read: op(A)[r][k] =
+//                 A[max(r,k)][min(r,k)] (ta is ignored)
 // GEMM_SPLIT computes the products in split precision instead of FP64: every operand value is
 // rounded to FP32 and split into three BF16 parts (x ~ h + m + l, 24 significant bits, the
 // width of FP32), and A B ~ the six products of significance down to 2^-16 (Al Bh + Am Bm +
 // Ah Bl, then Am Bh + Ah Bm, then Ah Bh) on the BF16 tensor cores (mma.sync m16n8k16), summed in
 // FP32 within each k-step of 16 and in FP64 across k-steps; the result is stored in FP64.
-constexpr int GT = 64, GK = 16;
-enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8, GEMM_B_LOWER = 16, GEMM_SPLIT = 32 };
+constexpr int GT = 64, GK = 16, GSTAGES = 4;
+enum { GEMM_A_LOWER = 1, GEMM_A_UPPER = 2, GEMM_B_UPPER = 4, GEMM_LOWER_TILES = 8, GEMM_B_LOWER = 16, GEMM_SPLIT = 32,
+       GEMM_A_SYMM = 64 };
 
-// One shared-memory work area per CTA, used in turn (never at the same time, each user starting
-// and ending at a CTA barrier) by the GEMM's staging buffers and the Cholesky's diagonal block.
+// One dynamic shared-memory work area per CTA, used in turn (never at the same time, each user
+// starting and ending at a CTA barrier): the GEMM's stages, the Cholesky's diagonal block, the
+// bisection's tridiagonal matrix, the band reduction's per-warp tiles and the second stage's
+// back-transformation blocks.
 constexpr int CB = 64;
-constexpr int SMEM_WORK = 2 * 2 * GK * (GT + 2);
-static_assert(CB * (CB + 1) <= SMEM_WORK, "diagonal block fits the GEMM staging area");
-__shared__ __align__(16) double s_work[SMEM_WORK];
+constexpr int GSTAGE = 2 * GK * (GT + 2);  // A and B tiles of one stage
+constexpr int SMEM_WORK = GSTAGES * GSTAGE;
+constexpr int SMEM_WORK_BYTES = SMEM_WORK * 8;
+static_assert(CB * (CB + 1) <= SMEM_WORK, "diagonal block fits the work area");
+extern __shared__ __align__(16) double s_work[];
 
 __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(c0), "+d"(c1)
                  : "d"(a), "d"(b));
 }
+
+// 8-byte asynchronous copy global -> shared; ok = false zero-fills the destination without a read
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool ok) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // two FP64 values -> three BF16 parts each (x ~ h + m + l after rounding to FP32), packed in
 // pairs as mma operands (the first value in the low half)
@@ -161,19 +178,14 @@ template <bool SPLIT>
 __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha,
                                          const double* A, long long lda, const double* B, long long ldb, double beta,
                                          double* Cm, long long ldc, int flags) {
-    auto& As = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work);
-    auto& Bs = *reinterpret_cast<double(*)[2][GK][GT + 2]>(s_work + 2 * GK * (GT + 2));
+    typedef double Stage[2][GK][GT + 2];  // [A, B][k][m or n]
+    Stage* stg = reinterpret_cast<Stage*>(s_work);
     if (M <= 0 || N <= 0) return;
+    const bool symm = (flags & GEMM_A_SYMM) != 0;
     int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int wm = warp & 1, wn = warp >> 1;  // warp block: rows wm*32.., cols wn*16..
     int lr = lane >> 2, lc = lane & 3;
-    // each thread stages 4 elements of each operand per k-step (element e = tid + 256 q, laid
-    // out along the operand's contiguous dimension)
-#define A_MM(q) (ta ? (int)(threadIdx.x + (q) * 256) / GK : (int)(threadIdx.x + (q) * 256) % GT)
-#define A_KK(q) (ta ? (int)(threadIdx.x + (q) * 256) % GK : (int)(threadIdx.x + (q) * 256) / GT)
-#define B_NN(q) (tb ? (int)(threadIdx.x + (q) * 256) % GT : (int)(threadIdx.x + (q) * 256) / GK)
-#define B_KK(q) (tb ? (int)(threadIdx.x + (q) * 256) / GT : (int)(threadIdx.x + (q) * 256) % GK)
     for (int tile = t.rank; tile < tm * tn; tile += t.size) {
         int bi = tile % tm, bj = tile / tm;
         if ((flags & GEMM_LOWER_TILES) && bj > bi) continue;
@@ -183,7 +195,8 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
         if (flags & GEMM_B_UPPER) ke = min(ke, col0 + GT);
         if (flags & GEMM_A_UPPER) kb = max(kb, (row0 / GK) * GK);
         if (flags & GEMM_B_LOWER) kb = max(kb, (col0 / GK) * GK);
-        double acc[4][2][2];  // FP64: 4 x 2 tiles of 8 x 8 per warp
+        int nk = ke > kb ? (ke - kb + GK - 1) / GK : 0;
+        double acc[4][2][2];   // FP64: 4 x 2 tiles of 8 x 8 per warp
         double accf[2][2][4];  // split: 2 x 2 tiles of 16 x 8 per warp (FP64 sum of FP32 k-step partials)
 #pragma unroll
         for (int i = 0; i < 4; i++)
@@ -195,33 +208,47 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
             for (int j = 0; j < 2; j++)
 #pragma unroll
                 for (int h = 0; h < 4; h++) accf[i][j][h] = 0.0;
-        double ra[4], rb[4];
-        auto load = [&](int k0) {
+        // the copies of k-step `it` into stage it % GSTAGES: each thread 4 elements of each
+        // operand, consecutive threads along the operand's contiguous dimension
+        auto issue = [&](int it) {
+            int k0 = kb + it * GK;
+            Stage& S = stg[it % GSTAGES];
+            // op(A) tile rows row0.., k k0..; the symmetric operand is read as stored below the
+            // diagonal and transposed above it (both coalesced), element by element on the diagonal
+            bool at = symm ? (k0 >= row0 + GT) : ta;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                int gr = row0 + A_MM(q), gk = k0 + A_KK(q);
-                ra[q] = (gr < M && gk < ke) ? (ta ? A[gk + (long long)gr * lda] : A[gr + (long long)gk * lda]) : 0.0;
-                int gc = col0 + B_NN(q), gk2 = k0 + B_KK(q);
-                rb[q] = (gc < N && gk2 < ke) ? (tb ? B[gc + (long long)gk2 * ldb] : B[gk2 + (long long)gc * ldb]) : 0.0;
+                int e = threadIdx.x + q * 256;
+                int mm = at ? e / GK : e % GT, kk = at ? e % GK : e / GT;
+                int gr = row0 + mm, gk = k0 + kk;
+                bool ok = gr < M && gk < ke;
+                long long off;
+                if (symm) off = gr >= gk ? gr + (long long)gk * lda : gk + (long long)gr * lda;
+                else off = ta ? gk + (long long)gr * lda : gr + (long long)gk * lda;
+                cp_async8(&S[0][kk][mm], ok ? A + off : A, ok);
             }
-        };
-        auto store = [&](int buf) {
 #pragma unroll
             for (int q = 0; q < 4; q++) {
-                As[buf][A_KK(q)][A_MM(q)] = ra[q];
-                Bs[buf][B_KK(q)][B_NN(q)] = rb[q];
+                int e = threadIdx.x + q * 256;
+                int nn = tb ? e % GT : e / GK, kk = tb ? e / GT : e % GK;
+                int gc = col0 + nn, gk = k0 + kk;
+                bool ok = gc < N && gk < ke;
+                long long off = tb ? gc + (long long)gk * ldb : gk + (long long)gc * ldb;
+                cp_async8(&S[1][kk][nn], ok ? B + off : B, ok);
             }
         };
-        __syncthreads();
-        int cur = 0;
-        if (kb < ke) {
-            load(kb);
-            store(0);
+        __syncthreads();  // the stages are free (the previous tile or user is done with them)
+#pragma unroll
+        for (int it = 0; it < GSTAGES - 1; it++) {
+            if (it < nk) issue(it);
+            cp_async_commit();
         }
-        __syncthreads();
-        for (int k0 = kb; k0 < ke; k0 += GK) {
-            bool more = k0 + GK < ke;
-            if (more) load(k0 + GK);
+        for (int it = 0; it < nk; it++) {
+            cp_async_wait<GSTAGES - 2>();  // this thread's copies of k-step it have landed
+            __syncthreads();               // everyone's have; and stage (it - 1) % GSTAGES is free
+            if (it + GSTAGES - 1 < nk) issue(it + GSTAGES - 1);
+            cp_async_commit();
+            Stage& S = stg[it % GSTAGES];
             if constexpr (SPLIT) {
                 // one k16 step: A rows g, g + 8 of each 16-row tile; k = 2 lc (+1), 2 lc + 8 (+1)
                 unsigned ah[2][4], am[2][4], al[2][4], bh[2][2], bm[2][2], bl[2][2];
@@ -229,16 +256,16 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
 #pragma unroll
                 for (int i = 0; i < 2; i++) {
                     int r = wm * 32 + i * 16 + lr;
-                    split_pair(As[cur][k0s][r], As[cur][k0s + 1][r], ah[i][0], am[i][0], al[i][0]);
-                    split_pair(As[cur][k0s][r + 8], As[cur][k0s + 1][r + 8], ah[i][1], am[i][1], al[i][1]);
-                    split_pair(As[cur][k0s + 8][r], As[cur][k0s + 9][r], ah[i][2], am[i][2], al[i][2]);
-                    split_pair(As[cur][k0s + 8][r + 8], As[cur][k0s + 9][r + 8], ah[i][3], am[i][3], al[i][3]);
+                    split_pair(S[0][k0s][r], S[0][k0s + 1][r], ah[i][0], am[i][0], al[i][0]);
+                    split_pair(S[0][k0s][r + 8], S[0][k0s + 1][r + 8], ah[i][1], am[i][1], al[i][1]);
+                    split_pair(S[0][k0s + 8][r], S[0][k0s + 9][r], ah[i][2], am[i][2], al[i][2]);
+                    split_pair(S[0][k0s + 8][r + 8], S[0][k0s + 9][r + 8], ah[i][3], am[i][3], al[i][3]);
                 }
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     int c = wn * 16 + j * 8 + lr;
-                    split_pair(Bs[cur][k0s][c], Bs[cur][k0s + 1][c], bh[j][0], bm[j][0], bl[j][0]);
-                    split_pair(Bs[cur][k0s + 8][c], Bs[cur][k0s + 9][c], bh[j][1], bm[j][1], bl[j][1]);
+                    split_pair(S[1][k0s][c], S[1][k0s + 1][c], bh[j][0], bm[j][0], bl[j][0]);
+                    split_pair(S[1][k0s + 8][c], S[1][k0s + 9][c], bh[j][1], bm[j][1], bl[j][1]);
                 }
                 // per k-step partial sum in FP32, smallest terms first, added to the accumulator
 #pragma unroll
@@ -260,21 +287,17 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
                 for (int kk = 0; kk < GK; kk += 4) {
                     double af[4], bf[2];
 #pragma unroll
-                    for (int i = 0; i < 4; i++) af[i] = As[cur][kk + lc][wm * 32 + i * 8 + lr];
+                    for (int i = 0; i < 4; i++) af[i] = S[0][kk + lc][wm * 32 + i * 8 + lr];
 #pragma unroll
-                    for (int j = 0; j < 2; j++) bf[j] = Bs[cur][kk + lc][wn * 16 + j * 8 + lr];
+                    for (int j = 0; j < 2; j++) bf[j] = S[1][kk + lc][wn * 16 + j * 8 + lr];
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
                         for (int j = 0; j < 2; j++) dmma_8x8x4(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
                 }
             }
-            if (more) {
-                store(cur ^ 1);
-                __syncthreads();
-                cur ^= 1;
-            }
         }
+        cp_async_wait<0>();
         if constexpr (SPLIT) {
 #pragma unroll
             for (int i = 0; i < 2; i++)
@@ -307,6 +330,7 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
             }
         }
     }
+    __syncthreads();  // the stages are free for the next user
 }
 
 __device__ __forceinline__ void team_gemm(const Team& t, bool ta, bool tb, int M, int N, int K, double alpha,
@@ -315,11 +339,6 @@ __device__ __forceinline__ void team_gemm(const Team& t, bool ta, bool tb, int M
     if (flags & GEMM_SPLIT) team_gemm_t<true>(t, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, Cm, ldc, flags);
     else team_gemm_t<false>(t, ta, tb, M, N, K, alpha, A, lda, B, ldb, beta, Cm, ldc, flags);
 }
-
-#undef A_MM
-#undef A_KK
-#undef B_NN
-#undef B_KK
 
 // A[c][i] = A[i][c] for i > c in the square block [r0, n)
 __device__ void team_mirror_lower(const Team& t, double* A, long long lda, int r0, int n) {
