@@ -448,7 +448,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         long long nt = (n + 31) / 32;
         ntiles += nt * nt;
         long long nw = std::max(n, 64LL);
-        nwk += (2LL + axg::symv_slots((int)n)) * nw + 64LL * nw + 2 * 64 * 64 + 2 * 64LL * nw + 64LL * nw + 64;
+        nwk += (axg::team_workspace((int)n) + 31) & ~31LL;
     }
     // atoms / shells / AOs
     vector<int> a_Z(natT), a_mol(natT), a_sh0(natT), a_nsh(natT), a_ao0(natT), a_sp(natT);
@@ -857,6 +857,9 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.max_iter = o.max_iter;
     b.split = o.precision == 1 ? 1 : 0;
     b.disp = o.dispersion ? 1 : 0;
+    // the two-stage tridiagonal reduction for one-CTA molecules (AXTB_EIGEN_ONESTAGE=1 selects the
+    // one-stage reduction the whole-grid molecules use, for comparisons)
+    b.band = std::getenv("AXTB_EIGEN_ONESTAGE") ? 0 : 1;
     // state
     axg::State& s = S;
     s.xyz = ar.take<double>(natT * 3);
@@ -1384,12 +1387,14 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
 namespace {
 constexpr int STATIC_MAX_NAO = 256;
 constexpr long long STATIC_PLANE = (long long)STATIC_MAX_NAO * STATIC_MAX_NAO;  // doubles per matrix
-constexpr long long STATIC_WK = 274LL * STATIC_MAX_NAO + 8192 + 64;             // team workspace
+constexpr long long STATIC_WK = axg::team_workspace(STATIC_MAX_NAO);             // team workspace
+static_assert(STATIC_WK >= axg::band_workspace(STATIC_MAX_NAO) && STATIC_WK >= axg::onestage_workspace(STATIC_MAX_NAO),
+              "the static workspace holds the eigen phase's layout at the largest molecule");
 constexpr long long STATIC_VEC = 8LL * STATIC_MAX_NAO;                           // d, e, tau + spare
 constexpr long long STATIC_PIV = STATIC_PLANE / 8;                               // pivot bytes, as doubles
 constexpr long long STATIC_PAR = 64;                                             // small parameters
-constexpr long long STATIC_DOUBLES = 7 * STATIC_PLANE + STATIC_WK + STATIC_VEC + STATIC_PIV + STATIC_PAR;
-static __device__ __align__(256) double g_density_scratch[STATIC_DOUBLES];  // 4.25 MiB
+constexpr long long STATIC_DOUBLES = 8 * STATIC_PLANE + STATIC_WK + STATIC_VEC + STATIC_PIV + STATIC_PAR;
+static __device__ __align__(256) double g_density_scratch[STATIC_DOUBLES];  // 4.89 MiB
 
 std::mutex g_static_mu;
 double* g_static_addr[256] = {nullptr};
@@ -1413,6 +1418,7 @@ __global__ void __launch_bounds__(TEAM_THREADS)
     Team one{0, 1, false};
     mol_overlap(one, B, S, P, 0);
     mol_eigen(one, B, S, P, 0);
+    mol_levels(one, B, S, P, 0);  // every orbital energy, not only the ones the filling needs
     if (threadIdx.x == 0 && d_status) *d_status = S.status[0];
 }
 }  // namespace axg
@@ -1472,6 +1478,7 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.C = take(STATIC_PLANE);
     S.scr2 = take(STATIC_PLANE);
     S.scr3 = take(STATIC_PLANE);
+    S.W = take(STATIC_PLANE);  // the band reduction's second-stage reflectors
     P.wk = take(STATIC_WK);
     double* vec = take(STATIC_VEC);
     S.dtri = vec;
@@ -1496,6 +1503,7 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.P = d_density;
     B.nmol = 1;
     B.kt = kt;
+    B.band = 1;
     axg::k_density_static<<<1, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta,
                                                                                               d_status);
     cudaError_t e = cudaGetLastError();

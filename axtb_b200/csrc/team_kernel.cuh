@@ -12,6 +12,7 @@
 #pragma once
 #include "common.cuh"
 #include "team_la.cuh"
+#include "team_band.cuh"
 
 namespace axg {
 
@@ -162,12 +163,20 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
     const int nsl = symv_slots(n);
-    {
+    const bool band = !t.global && B.band;
+    if (band) {
+        // one CTA: two-stage reduction (dense -> band on GEMMs, band -> tridiagonal by bulge
+        // chasing), the stage-2 reflectors in the W plane (free until the gradient's W)
+        team_sy2sb(t, Fp, n, n, tau, wk);
+        TEAM_PHASE(8);
+        team_sb2st(t, Fp, n, n, d, e, wk, S.W + mat);
+        TEAM_PHASE(10);
+    } else {
         double* Vp = wk + 2 * n + (long long)nsl * n;  // the back-transform's vb area (64 n)
         team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
                              P.cycles != 0);
+        if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     }
-    if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     TEAM_PHASE(1);
     double* emo = S.emo + ao0;
     // eigenvalues: the lowest ceil(n_occ) + a margin first; the levels above get the Gershgorin
@@ -199,7 +208,12 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* gm = tb + 64 * 64;
     double* y = gm + 64 * 64;
     double* y2 = y + 64LL * n;
-    team_backtransform(t, Fp, n, tau, n, k, Zm, n, vb, tb, gm, y, y2);
+    if (band) {
+        team_apply_q2(t, n, k, Zm, n, S.W + mat, wk);
+        team_apply_q1(t, Fp, n, n, k, Zm, n, wk);
+    } else {
+        team_backtransform(t, Fp, n, tau, n, k, Zm, n, vb, tb, gm, y, y2);
+    }
     TEAM_PHASE(5);
     // C = L^-T Z'; P = (C f) C^T
     double* Cm = S.C + mat;

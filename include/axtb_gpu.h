@@ -207,7 +207,7 @@ void axtb_gpu_batch_destroy(AxtbBatch* b);
  * allocating any device memory. No counterpart in the reference: it is for callers that cannot
  * call cudaMalloc, e.g. code inside another framework's stream-ordered memory pool or under a
  * fixed device-memory budget, where an allocation would fail or would synchronise the device.
- * All scratch lives in one array in the library's device image: 4.25 MiB, held by every GPU
+ * All scratch lives in one array in the library's device image: 4.89 MiB, held by every GPU
  * that loads the library until the process exits, which limits nao to 256.
  * Inputs d_fock and d_overlap (nao*nao, column-major) and outputs d_emo, d_focc (nao) and
  * d_density (nao*nao) are device pointers the caller allocates; d_status (optional, device)
