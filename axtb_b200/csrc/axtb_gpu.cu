@@ -1241,7 +1241,11 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
         CK(cudaMemsetAsync(P.eeq_q, 0, sizeof(double) * natT, st));
         LAUNCH("d4_weights", 0, 0, k_d4_weights<<<blocks_for(natT, T), T, 0, st>>>(B, S, P.eeq_q, 1));
         LAUNCH("atm_tables", 0, 0, k_atm_tables<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, nsqT));
-        LAUNCH("atm", 0, 0, k_atm<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0));
+        if (npairT > 0)
+            LAUNCH("atm", 0, 0,
+                   k_atm_pairs<<<blocks_for(npairT * 32, T), T, 0, st>>>(B, S, d_wt, d_tt, d_sq0, d_pair0, npairT,
+                                                                        S.pair_buf));
+        LAUNCH("atm_gather", 0, 0, k_atm_gather<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S, d_pair0, S.pair_buf));
         LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, d_eatm));
     } else {
         CK(cudaMemsetAsync(d_eatm, 0, sizeof(double) * nmol, st));

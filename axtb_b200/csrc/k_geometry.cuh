@@ -267,19 +267,78 @@ __global__ void k_atm_tables(Batch B, State S, double* wt, double* tt, const lon
     tt[m_sq0[m] + gi] = tv;
 }
 
-// ATM energy, gradient and dE/dCN (D4 CN) per atom in the pair-sum form of the axtb conventions
-// (crates/d4/src/disp.rs:666-733 and its term kernel 920-960): atom a sums, over its partners b,
-// the pair's sum over third atoms k. One warp per atom, lanes over k.
-__global__ void k_atm(Batch B, State S, const double* wt, const double* tt, const long long* m_sq0) {
+// ATM in the pair-sum form of the axtb conventions (crates/d4/src/disp.rs:666-733 and its term
+// kernel 920-960): for every atom pair (a, b) the sum over third atoms k of the triple's damped
+// angular term (ds) and its radial derivative (gs). Both sums are symmetric in a and b, so each
+// unordered pair (a > b) is summed once, by one warp with lanes over k, into pairs[2 p]; the
+// gather below turns them into each atom's energy, gradient and dE/dCN.
+__global__ void k_atm_pairs(Batch B, State S, const double* wt, const double* tt, const long long* m_sq0,
+                            const long long* m_pair0, long long np, double* pairs) {
+    long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (p >= np) return;
+    int m = find_mol(m_pair0, B.nmol, p);
+    long long pl = p - m_pair0[m];
+    int la = (int)((sqrt(8.0 * (double)pl + 1.0) + 1.0) * 0.5);  // pl = la (la - 1) / 2 + lb, lb < la
+    while ((long long)la * (la - 1) / 2 > pl) la--;
+    while ((long long)(la + 1) * la / 2 <= pl) la++;
+    int lb = (int)(pl - (long long)la * (la - 1) / 2);
+    int n = B.m_nat[m], i0 = B.m_at0[m];
+    int a = i0 + la, b = i0 + lb;
+    double ds = 0.0, gs = 0.0;
+    double vab[3];
+    dvec(S.xyz, b, a, vab);
+    double r2 = vab[0] * vab[0] + vab[1] * vab[1] + vab[2] * vab[2];
+    if (r2 <= B.d3_cut * B.d3_cut && r2 >= DBL_EPSILON) {
+        const double* W = wt + m_sq0[m];
+        const double* T = tt + m_sq0[m];
+        const double alp3 = D4_ALP / 3.0;
+        double ir = 1.0 / sqrt(r2), t6 = 6.0 * T[(long long)la * n + lb];
+        double r2_2 = r2 * r2;
+        const double* wa = W + (long long)la * n;
+        const double* wb = W + (long long)lb * n;
+        const double* ta = T + (long long)la * n;
+        const double* tb = T + (long long)lb * n;
+        for (int lk = lane; lk < n; lk += 32) {
+            double c = wa[lk] * wb[lk];
+            if (c == 0.0) continue;
+            int k = i0 + lk;
+            double vak[3], vbk[3];
+            dvec(S.xyz, k, a, vak);
+            dvec(S.xyz, k, b, vbk);
+            double r2ak = vak[0] * vak[0] + vak[1] * vak[1] + vak[2] * vak[2];
+            double r2bk = vbk[0] * vbk[0] + vbk[1] * vbk[1] + vbk[2] * vbk[2];
+            double cralp = t6 * ta[lk] * tb[lk];
+            double fdmp = 1.0 / (1.0 + cralp);
+            double ir1 = ir / (sqrt(r2ak) * sqrt(r2bk));
+            double rrr2 = ir1 * ir1, rrr3 = rrr2 * ir1;
+            double angf = 0.375 * rrr2 * rrr3;
+            double s1 = r2ak + r2bk, d1 = (r2bk - r2ak) * (r2bk - r2ak);
+            double ang = angf * ((r2_2 - d1) * (s1 - r2)) + rrr3;
+            double cf = c * fdmp;
+            ds += ang * cf;
+            double pp = r2 * (r2 * (r2 + s1) + 2.0 * (s1 * s1) + d1) - 5.0 * (d1 * s1);
+            gs += cf * (angf * pp - alp3 * (cralp * fdmp) * ang);
+        }
+        ds = warp_sum(ds);
+        gs = warp_sum(gs);
+    }
+    if (lane == 0) {
+        pairs[2 * p] = ds;
+        pairs[2 * p + 1] = gs;
+    }
+}
+
+// ATM energy, gradient and dE/dCN (D4 CN) per atom from the pair sums: atom a adds, over its
+// partners b, -sw d / 6, the radial force and -d sw dC6/dCN_a / (2 C6), with
+// d = -s9 sqrt|C6_ab| ds. One warp per atom, lanes over partners.
+__global__ void k_atm_gather(Batch B, State S, const long long* m_pair0, const double* pairs) {
     int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (a >= B.natT) return;
     AtomView mv = mol_atoms(B, a);
     int n = mv.n, la = a - mv.i0;
-    const double* W = wt + m_sq0[mv.m];
-    const double* T = tt + m_sq0[mv.m];
-    const double alp3 = D4_ALP / 3.0;
     double ea = 0.0, ga[3] = {0, 0, 0}, dca = 0.0;
-    for (int lb = 0; lb < n; lb++) {
+    for (int lb = lane; lb < n; lb += 32) {
         if (lb == la) continue;
         int b = mv.i0 + lb;
         double vab[3];
@@ -289,33 +348,9 @@ __global__ void k_atm(Batch B, State S, const double* wt, const double* tt, cons
         double r = sqrt(r2), sw, dsw;
         smooth_cut(r, B.d3_cut, B.d3_w, sw, dsw);
         if (sw <= 0.0) continue;
-        double ir = 1.0 / r, t6 = 6.0 * T[(long long)la * n + lb];
-        double r2_2 = r2 * r2;
-        double gs = 0.0, ds = 0.0;
-        for (int lk = lane; lk < n; lk += 32) {
-            double wak = W[(long long)la * n + lk], wbk = W[(long long)lb * n + lk];
-            double c = wak * wbk;
-            if (c == 0.0) continue;
-            int k = mv.i0 + lk;
-            double vak[3], vbk[3];
-            dvec(S.xyz, k, a, vak);
-            dvec(S.xyz, k, b, vbk);
-            double r2ak = vak[0] * vak[0] + vak[1] * vak[1] + vak[2] * vak[2];
-            double r2bk = vbk[0] * vbk[0] + vbk[1] * vbk[1] + vbk[2] * vbk[2];
-            double cralp = t6 * T[(long long)la * n + lk] * T[(long long)lb * n + lk];
-            double fdmp = 1.0 / (1.0 + cralp);
-            double ir1 = ir / (sqrt(r2ak) * sqrt(r2bk));
-            double rrr2 = ir1 * ir1, rrr3 = rrr2 * ir1;
-            double angf = 0.375 * rrr2 * rrr3;
-            double s1 = r2ak + r2bk, d1 = (r2bk - r2ak) * (r2bk - r2ak);
-            double ang = angf * ((r2_2 - d1) * (s1 - r2)) + rrr3;
-            double cf = c * fdmp;
-            ds += ang * cf;
-            double p = r2 * (r2 * (r2 + s1) + 2.0 * (s1 * s1) + d1) - 5.0 * (d1 * s1);
-            gs += cf * (angf * p - alp3 * (cralp * fdmp) * ang);
-        }
-        ds = warp_sum(ds);
-        gs = warp_sum(gs);
+        long long pl = la > lb ? (long long)la * (la - 1) / 2 + lb : (long long)lb * (lb - 1) / 2 + la;
+        const double* pp = pairs + 2 * (m_pair0[mv.m] + pl);
+        double ds = pp[0], gs = pp[1];
         double c6, dda, ddb;
         pair_c6(B, S, a, b, c6, dda, ddb);
         double cab = -(D4_S9 * sqrt(fabs(c6)));
@@ -327,6 +362,9 @@ __global__ void k_atm(Batch B, State S, const double* wt, const double* tt, cons
         double qa = c6 != 0.0 ? dda / c6 : 0.0;
         dca -= 0.5 * de * qa;
     }
+    ea = warp_sum(ea);
+    dca = warp_sum(dca);
+    for (int x = 0; x < 3; x++) ga[x] = warp_sum(ga[x]);
     if (lane == 0) {
         S.e_atom[a] += ea;
         for (int x = 0; x < 3; x++) S.grad[3 * a + x] += ga[x];

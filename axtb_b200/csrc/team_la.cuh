@@ -802,10 +802,140 @@ __device__ void team_gershgorin(const Team& t, const double* d, const double* e,
     t.sync();
 }
 
+// Sturm counts of R shifts at once (independent recurrences interleaved, so the divisions of one
+// hide the latency of the others), d and e^2 in shared memory
+template <int R>
+__device__ __forceinline__ void sturm_counts_sh(const double* sd, const double* se2, int n, const double* x,
+                                                double pivmin, int* cnt) {
+    double q[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        q[r] = sd[0] - x[r];
+        if (fabs(q[r]) < pivmin) q[r] = -pivmin;
+        cnt[r] = q[r] < 0.0 ? 1 : 0;
+    }
+    for (int i = 1; i < n; i++) {
+        double di = sd[i], ei = se2[i - 1];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            q[r] = di - x[r] - ei / q[r];
+            if (fabs(q[r]) < pivmin) q[r] = -pivmin;
+            cnt[r] += q[r] < 0.0 ? 1 : 0;
+        }
+    }
+}
+
+__device__ __forceinline__ bool bisect_done(double lo, double hi, double pivmin) {
+    return hi - lo <= 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)) + pivmin;
+}
+
+// R eigenvalues per thread (k = k0 + threadIdx.x + r blockDim.x), bisection interleaved
+template <int R>
+__device__ void cta_bisect_ilp(const double* sd, const double* se2, int n, double* w, double glo, double ghi,
+                               double pivmin, int k0, int k1) {
+    double lo[R], hi[R], x[R];
+    int cnt[R];
+    bool live[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        lo[r] = glo;
+        hi[r] = ghi;
+        live[r] = k0 + (int)threadIdx.x + r * (int)blockDim.x < k1;
+    }
+    for (int it = 0; it < 200; it++) {
+        bool any = false;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            double mid = 0.5 * (lo[r] + hi[r]);
+            if (live[r] && (bisect_done(lo[r], hi[r], pivmin) || mid <= lo[r] || mid >= hi[r])) live[r] = false;
+            x[r] = live[r] ? mid : lo[r];
+            any = any || live[r];
+        }
+        if (!any) break;
+        sturm_counts_sh<R>(sd, se2, n, x, pivmin, cnt);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            int k = k0 + (int)threadIdx.x + r * (int)blockDim.x;
+            if (!live[r]) continue;
+            if (cnt[r] > k) hi[r] = x[r];
+            else lo[r] = x[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        int k = k0 + (int)threadIdx.x + r * (int)blockDim.x;
+        if (k < k1) w[k] = 0.5 * (lo[r] + hi[r]);
+    }
+}
+
+// one eigenvalue per group of g lanes (g a power of two <= 32): each step the group's lanes
+// evaluate the Sturm count at g interior points of the bracket, which shrinks to the (g+1)-th
+// part holding the eigenvalue (log2(g+1) bits per step instead of one)
+__device__ void cta_bisect_groups(const double* sd, const double* se2, int n, double* w, double glo, double ghi,
+                                  double pivmin, int k0, int k1, int g) {
+    int lane = threadIdx.x & 31, gl = lane % g, base = lane - gl;
+    unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << base);
+    int k = k0 + (int)threadIdx.x / g;
+    bool live = k < k1;
+    double lo = glo, hi = ghi;
+    for (int it = 0; it < 200; it++) {
+        double h = (hi - lo) / (double)(g + 1);
+        double xf = lo + h, xl = lo + (double)g * h;
+        if (live && (bisect_done(lo, hi, pivmin) || !(xf > lo && xl < hi))) live = false;
+        if (!__any_sync(0xffffffffu, live)) break;
+        double x = lo + (double)(gl + 1) * h;
+        int c = 0;
+        if (live) sturm_counts_sh<1>(sd, se2, n, &x, pivmin, &c);
+        unsigned below = __ballot_sync(0xffffffffu, live && c <= k) & gmask;
+        int j = __popc(below);  // points at or below the eigenvalue: a prefix of the group
+        double xlo = __shfl_sync(0xffffffffu, x, base + max(j - 1, 0));
+        double xhi = __shfl_sync(0xffffffffu, x, base + min(j, g - 1));
+        if (live) {
+            if (j > 0) lo = xlo;
+            if (j < g) hi = xhi;
+        }
+    }
+    if (k < k1 && gl == 0) w[k] = 0.5 * (lo + hi);
+}
+
+// eigenvalues k0..k1-1 of one CTA's tridiagonal (d, e), d and e^2 staged in shared memory
+__device__ void cta_bisect(const double* d, const double* e, int n, double* w, const double* gbuf, int k0, int k1) {
+    double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
+    double* sd = s_work;
+    double* se2 = s_work + n;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sd[i] = d[i];
+        se2[i] = i + 1 < n ? e[i] * e[i] : 0.0;
+    }
+    __syncthreads();
+    int cnt = k1 - k0, nt = blockDim.x;
+    if (cnt > 0) {
+        if (cnt <= nt / 2) {
+            int g = 2;
+            while (g < 32 && nt / (2 * g) >= cnt) g *= 2;
+            cta_bisect_groups(sd, se2, n, w, glo, ghi, pivmin, k0, k1, g);
+        } else if (cnt <= nt) {
+            cta_bisect_ilp<1>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
+        } else if (cnt <= 2 * nt) {
+            cta_bisect_ilp<2>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
+        } else if (cnt <= 3 * nt) {
+            cta_bisect_ilp<3>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
+        } else {
+            cta_bisect_ilp<4>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
+        }
+    }
+    __syncthreads();
+}
+
 // eigenvalues k0..k1-1 (ascending order) by bisection, one thread per eigenvalue index; gbuf holds
-// team_gershgorin's bounds
+// team_gershgorin's bounds. One CTA whose matrix fits the shared work area: cta_bisect.
 __device__ __noinline__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w,
                                          const double* gbuf, int k0, int k1) {
+    if (!t.global && 2 * n <= SMEM_WORK && k1 - k0 <= 4 * (int)blockDim.x) {
+        cta_bisect(d, e, n, w, gbuf, k0, k1);
+        return;
+    }
     double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
     for (int k = k0 + t.tid(); k < k1; k += t.nthreads()) {
         double lo = glo, hi = ghi;
