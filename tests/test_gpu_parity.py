@@ -60,11 +60,14 @@ def test_batch_equals_single_and_oracle(engine):
 
     mols = S.mixed_batch(24, seed=11)
     res = engine.Batch(mols, accuracy=1e-6).run(gradient=True)
-    for (z, x), r in zip(mols[:6], res[:6]):
-        ref = O.singlepoint(z, x, accuracy=1e-6)
+    for (z, x), r in zip(mols, res):
+        ref = O.singlepoint(z, x, accuracy=1e-6, lapack=True, lapack_threads=4)
         assert r.status == 0
         assert abs(r.energy - ref["energy"]) < E_TOL
         assert np.abs(r.gradient - ref["gradient"]).max() < G_TOL
+        assert np.abs(r.charges - ref["qat"]).max() < 1e-7
+    single = engine.Calculator(*mols[1], accuracy=1e-6).singlepoint(mols[1][1])
+    assert abs(single.energy - res[1].energy) < 1e-12
 
 
 def test_grid_team_path_matches_oracle(engine, golden, monkeypatch):

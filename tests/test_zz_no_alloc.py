@@ -1,5 +1,5 @@
 """The allocation-free density entry point (axtb_gpu_density_static) against the engine's own
-results (GPU).
+results and an independent generalized eigensolve (GPU).
 
 Some callers cannot allocate device memory: code that runs inside another framework's
 stream-ordered memory pool, or under a fixed device-memory budget, where cudaMalloc would
@@ -10,7 +10,9 @@ runs a molecule through the ordinary batch entry points, reads back the last Foc
 matrices with the orbital energies, occupations and density they produced, feeds the two
 matrices to the allocation-free entry point through the C ABI and compares its outputs, on
 consecutive calls that reuse the shared scratch array (the last one repeating the first
-molecule after a different one has left its contents behind).
+molecule after a different one has left its contents behind); at the documented maximum of 256
+basis functions its outputs are also checked against scipy's generalized eigensolver with a
+Fermi filling of its own.
 
 This file is named to be collected last, so that a run stopping at its first failure has
 already run every other test; it also passes alone in a fresh process.
@@ -28,7 +30,7 @@ TOL = 1e-10
 
 def _engine_case(engine, z, x):
     b = engine.Batch([(z, x)], accuracy=1e-6)
-    b.run(gradient=False)
+    b.run(gradient=False, levels=True)
     case = {k: b.debug(0, k) for k in ("fock", "overlap", "emo", "focc", "density")}
     b.close()
     return case
@@ -68,6 +70,45 @@ def test_density_static_matches_engine(engine):
         assert np.abs(emo - case["emo"]).max() < TOL
         assert np.abs(focc - case["focc"]).max() < TOL
         assert np.abs(dens - case["density"]).max() < TOL
+
+
+def _fermi(eps, nel, kt):
+    """Occupations (0..2) of the levels eps holding nel electrons at kT, by bisection on the
+    chemical potential (an independent filling, not the engine's Newton iteration)."""
+    lo, hi = eps[0] - 10.0, eps[-1] + 10.0
+    for _ in range(200):
+        mu = 0.5 * (lo + hi)
+        f = 2.0 / (1.0 + np.exp(np.clip((eps - mu) / kt, -700, 700)))
+        if f.sum() > nel:
+            hi = mu
+        else:
+            lo = mu
+    return 2.0 / (1.0 + np.exp(np.clip((eps - 0.5 * (lo + hi)) / kt, -700, 700)))
+
+
+def test_density_static_at_its_maximum_matches_scipy(engine):
+    """C42H86 (254 basis functions, near the 256 limit): orbital energies, occupations and
+    density from a plain generalized eigensolve F C = S C e (scipy.linalg.eigh), on two calls."""
+    import scipy.linalg
+    import torch
+
+    from axtb_b200 import _lib, structures
+
+    lib = _lib.load()
+    case = _engine_case(engine, *structures.alkane(42, seed=3))
+    nao = len(case["emo"])
+    assert 250 <= nao <= 256
+    F, S = case["fock"], case["overlap"]
+    eps, C = scipy.linalg.eigh(0.5 * (F + F.T), 0.5 * (S + S.T))
+    nel = float(case["focc"].sum())
+    f = _fermi(eps, nel, 300.0 * KB_HARTREE)
+    P = (C * f) @ C.T
+    for _ in range(2):
+        emo, focc, dens, status = _static_call(lib, torch, case)
+        assert status == 0
+        assert np.abs(emo - eps).max() < 1e-9
+        assert np.abs(focc - f).max() < 1e-8
+        assert np.abs(dens - P).max() < 1e-8
 
 
 def test_density_static_rejects_oversize(engine):
