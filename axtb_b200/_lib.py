@@ -28,7 +28,8 @@ class AxtbOptions(C.Structure):
     _fields_ = [("accuracy", C.c_double), ("etemp", C.c_double), ("max_iter", C.c_int32), ("damping", C.c_double),
                 ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("mixer", C.c_int32),
                 ("conventions", C.c_int32), ("solvation", C.c_int32), ("solvent", C.c_char_p),
-                ("solvation_state", C.c_int32), ("dispersion", C.c_int32)]
+                ("solvation_state", C.c_int32), ("dispersion", C.c_int32),
+                ("band_min_nao", C.c_int32), ("grid_min_nao", C.c_int32)]
 
 
 class AxtbResult(C.Structure):

@@ -163,7 +163,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
     const int nsl = symv_slots(n);
-    const bool band = !t.global && B.band;
+    const bool band = !t.global && n >= B.band_min;
     if (band) {
         // one CTA: two-stage reduction (dense -> band on GEMMs, band -> tridiagonal by bulge
         // chasing), the stage-2 reflectors in the W plane (free until the gradient's W)

@@ -171,3 +171,24 @@ def test_input_errors(engine):
     with pytest.raises(AxtbError) as e:
         calc.singlepoint(np.full((3, 3), np.nan))
     assert e.value.kind == "input"
+
+
+def test_autotuned_schedule_gives_the_same_results(engine, tmp_path, monkeypatch):
+    """The autotuner (axtb_b200.autotune) measures the two-stage crossover and the whole-grid
+    threshold on a sample; any schedule gives the same energies and gradients to round-off."""
+    from axtb_b200 import autotune
+    from axtb_b200 import structures as S
+
+    monkeypatch.setenv("AXTB_TUNE_CACHE", str(tmp_path))
+    mols = S.mixed_batch(48, seed=21)
+    res = autotune.tune(mols, accuracy=1e-6)
+    opts = res["options"]
+    assert opts == autotune.schedule()
+    assert 0 <= opts["band_min_nao"] and opts["grid_min_nao"] >= 512
+    base = engine.Batch(mols, accuracy=1e-6).run(gradient=True)
+    for sched in (opts, {"band_min_nao": 1 << 30}, {"band_min_nao": 0, "grid_min_nao": 200}):
+        other = engine.Batch(mols, accuracy=1e-6, **sched).run(gradient=True)
+        for a, b in zip(base, other):
+            assert a.status == b.status == 0
+            assert abs(a.energy - b.energy) < E_TOL
+            assert np.abs(a.gradient - b.gradient).max() < G_TOL
