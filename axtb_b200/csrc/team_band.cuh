@@ -209,13 +209,6 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
     int lo = j + 1 + s * BW, hi = min(lo + BW - 1, n - 1), L = hi - lo + 1;
     int pc = s == 0 ? j : lo - BW;
     int elo = hi + 1, ehi = min(hi + BW, n - 1), LE = ehi - elo + 1;  // block below (LE <= 0: none)
-    // the band columns of this window (its diagonal block and the block below) into L1 while the
-    // reflector is formed and applied to the tile
-    if (lane < L) {
-        const char* col = reinterpret_cast<const char*>(bd + (long long)(lo + lane) * LDB);
-#pragma unroll
-        for (int q = 0; q < 5; q++) asm volatile("prefetch.global.L1 [%0];" ::"l"(col + 128 * q));
-    }
     // the column to annihilate: column j (s = 0) or the tile's first column
     double x = 0.0;
     if (lane < L) x = s == 0 ? *band_at(bd, lo + lane, j) : Tl[lane][0];
@@ -254,9 +247,19 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
     if (tc == 0.0 && LE <= 0) return;
     __syncwarp();
     // the diagonal block lo..hi, two-sided: y = tau D v, w = y - tau/2 (v.y) v, D -= v w^T + w v^T
+    // (loads in batches of 16 independent ones per lane)
     if (lane < L) {
-        for (int r = 0; r < L; r++)
-            Tl[r][lane] = r >= lane ? *band_at(bd, lo + r, lo + lane) : *band_at(bd, lo + lane, lo + r);
+#pragma unroll
+        for (int r0 = 0; r0 < BW; r0 += 16) {
+            double tv[16];
+#pragma unroll
+            for (int u = 0; u < 16; u++) {
+                int r = r0 + u;
+                tv[u] = r < L ? (r >= lane ? *band_at(bd, lo + r, lo + lane) : *band_at(bd, lo + lane, lo + r)) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 16; u++) Tl[r0 + u][lane] = tv[u];
+        }
     }
     __syncwarp();
     if (tc != 0.0) {
@@ -278,8 +281,19 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
     }
     // the block below (rows elo..ehi, columns lo..hi) from the right; it stays in the tile
     if (LE > 0) {
-        if (lane < L)
-            for (int r = 0; r < LE; r++) Tl[r][lane] = *band_at(bd, elo + r, lo + lane);
+        if (lane < L) {
+#pragma unroll
+            for (int r0 = 0; r0 < BW; r0 += 16) {
+                double tv[16];
+#pragma unroll
+                for (int u = 0; u < 16; u++) {
+                    int r = r0 + u;
+                    tv[u] = r < LE ? *band_at(bd, elo + r, lo + lane) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 16; u++) Tl[r0 + u][lane] = tv[u];
+            }
+        }
         __syncwarp();
         if (lane < LE && tc != 0.0) {
             double u = 0.0;

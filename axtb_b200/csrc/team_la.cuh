@@ -182,22 +182,85 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
     Stage* stg = reinterpret_cast<Stage*>(s_work);
     if (M <= 0 || N <= 0) return;
     const bool symm = (flags & GEMM_A_SYMM) != 0;
-    int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT;
+    const int tm = (M + GT - 1) / GT, tn = (N + GT - 1) / GT, ntile = tm * tn;
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int wm = warp & 1, wn = warp >> 1;  // warp block: rows wm*32.., cols wn*16..
     int lr = lane >> 2, lc = lane & 3;
-    for (int tile = t.rank; tile < tm * tn; tile += t.size) {
-        int bi = tile % tm, bj = tile / tm;
-        if ((flags & GEMM_LOWER_TILES) && bj > bi) continue;
-        int row0 = bi * GT, col0 = bj * GT;
-        int kb = 0, ke = K;
+    // this CTA's tiles in order (tile = rank + i * size, upper tiles skipped for GEMM_LOWER_TILES)
+    // and each tile's k range; the k-steps of all of them form one stream, so the copies of the
+    // next tile's first k-steps are in flight while the current tile finishes and stores
+    auto next_tile = [&](int tile) {
+        for (tile += t.size; tile < ntile; tile += t.size)
+            if (!((flags & GEMM_LOWER_TILES) && tile / tm > tile % tm)) break;
+        return tile;
+    };
+    auto krange = [&](int tile, int& kb, int& nk) {
+        int row0 = (tile % tm) * GT, col0 = (tile / tm) * GT;
+        int k0 = 0, ke = K;
         if (flags & GEMM_A_LOWER) ke = min(ke, row0 + GT);
         if (flags & GEMM_B_UPPER) ke = min(ke, col0 + GT);
-        if (flags & GEMM_A_UPPER) kb = max(kb, (row0 / GK) * GK);
-        if (flags & GEMM_B_LOWER) kb = max(kb, (col0 / GK) * GK);
-        int nk = ke > kb ? (ke - kb + GK - 1) / GK : 0;
-        double acc[4][2][2];   // FP64: 4 x 2 tiles of 8 x 8 per warp
-        double accf[2][2][4];  // split: 2 x 2 tiles of 16 x 8 per warp (FP64 sum of FP32 k-step partials)
+        if (flags & GEMM_A_UPPER) k0 = max(k0, (row0 / GK) * GK);
+        if (flags & GEMM_B_LOWER) k0 = max(k0, (col0 / GK) * GK);
+        kb = k0;
+        nk = ke > k0 ? (ke - k0 + GK - 1) / GK : 1;  // an empty range: one k-step of zeros
+        return ke;
+    };
+    int first = t.rank;
+    if (first < ntile && (flags & GEMM_LOWER_TILES) && first / tm > first % tm) first = next_tile(first);
+    // the copies of one k-step of `tile` into `slot`: each thread 4 elements of each operand,
+    // consecutive threads along the operand's contiguous dimension; zero outside [kb, ke)
+    auto issue = [&](int tile, int k0, int ke, int slot) {
+        int row0 = (tile % tm) * GT, col0 = (tile / tm) * GT;
+        Stage& S = stg[slot];
+        // op(A) tile rows row0.., k k0..; the symmetric operand is read as stored below the
+        // diagonal and transposed above it (both coalesced), element by element on the diagonal
+        bool at = symm ? (k0 >= row0 + GT) : ta;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int e = threadIdx.x + q * 256;
+            int mm = at ? e / GK : e % GT, kk = at ? e % GK : e / GT;
+            int gr = row0 + mm, gk = k0 + kk;
+            bool ok = gr < M && gk < ke;
+            long long off;
+            if (symm) off = gr >= gk ? gr + (long long)gk * lda : gk + (long long)gr * lda;
+            else off = ta ? gk + (long long)gr * lda : gr + (long long)gk * lda;
+            cp_async8(&S[0][kk][mm], ok ? A + off : A, ok);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int e = threadIdx.x + q * 256;
+            int nn = tb ? e % GT : e / GK, kk = tb ? e / GT : e % GK;
+            int gc = col0 + nn, gk = k0 + kk;
+            bool ok = gc < N && gk < ke;
+            long long off = tb ? gc + (long long)gk * ldb : gk + (long long)gc * ldb;
+            cp_async8(&S[1][kk][nn], ok ? B + off : B, ok);
+        }
+    };
+    // issue cursor (runs GSTAGES - 1 k-steps ahead) and compute cursor
+    int it_tile = first, it_kb = 0, it_nk = 0, it_ke = 0, it_ks = 0;
+    if (it_tile < ntile) it_ke = krange(it_tile, it_kb, it_nk);
+    auto issue_next = [&](int slot) {
+        if (it_tile >= ntile) return;
+        issue(it_tile, it_kb + it_ks * GK, it_ke, slot);
+        if (++it_ks == it_nk) {
+            it_tile = next_tile(it_tile);
+            it_ks = 0;
+            if (it_tile < ntile) it_ke = krange(it_tile, it_kb, it_nk);
+        }
+    };
+    double acc[4][2][2];   // FP64: 4 x 2 tiles of 8 x 8 per warp
+    double accf[2][2][4];  // split: 2 x 2 tiles of 16 x 8 per warp (FP64 sum of FP32 k-step partials)
+    __syncthreads();  // the stages are free (the previous user is done with them)
+#pragma unroll
+    for (int st = 0; st < GSTAGES - 1; st++) {
+        issue_next(st);
+        cp_async_commit();
+    }
+    int f = 0;  // k-steps computed so far (the stage ring position)
+    for (int tile = first; tile < ntile; tile = next_tile(tile)) {
+        int kb_, nk;
+        krange(tile, kb_, nk);
+        int row0 = (tile % tm) * GT, col0 = (tile / tm) * GT;
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -208,47 +271,12 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
             for (int j = 0; j < 2; j++)
 #pragma unroll
                 for (int h = 0; h < 4; h++) accf[i][j][h] = 0.0;
-        // the copies of k-step `it` into stage it % GSTAGES: each thread 4 elements of each
-        // operand, consecutive threads along the operand's contiguous dimension
-        auto issue = [&](int it) {
-            int k0 = kb + it * GK;
-            Stage& S = stg[it % GSTAGES];
-            // op(A) tile rows row0.., k k0..; the symmetric operand is read as stored below the
-            // diagonal and transposed above it (both coalesced), element by element on the diagonal
-            bool at = symm ? (k0 >= row0 + GT) : ta;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                int e = threadIdx.x + q * 256;
-                int mm = at ? e / GK : e % GT, kk = at ? e % GK : e / GT;
-                int gr = row0 + mm, gk = k0 + kk;
-                bool ok = gr < M && gk < ke;
-                long long off;
-                if (symm) off = gr >= gk ? gr + (long long)gk * lda : gk + (long long)gr * lda;
-                else off = ta ? gk + (long long)gr * lda : gr + (long long)gk * lda;
-                cp_async8(&S[0][kk][mm], ok ? A + off : A, ok);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                int e = threadIdx.x + q * 256;
-                int nn = tb ? e % GT : e / GK, kk = tb ? e / GT : e % GK;
-                int gc = col0 + nn, gk = k0 + kk;
-                bool ok = gc < N && gk < ke;
-                long long off = tb ? gc + (long long)gk * ldb : gk + (long long)gc * ldb;
-                cp_async8(&S[1][kk][nn], ok ? B + off : B, ok);
-            }
-        };
-        __syncthreads();  // the stages are free (the previous tile or user is done with them)
-#pragma unroll
-        for (int it = 0; it < GSTAGES - 1; it++) {
-            if (it < nk) issue(it);
+        for (int ks = 0; ks < nk; ks++, f++) {
+            cp_async_wait<GSTAGES - 2>();  // this thread's copies of k-step f have landed
+            __syncthreads();               // everyone's have; and the stage of k-step f - 1 is free
+            issue_next((f + GSTAGES - 1) % GSTAGES);
             cp_async_commit();
-        }
-        for (int it = 0; it < nk; it++) {
-            cp_async_wait<GSTAGES - 2>();  // this thread's copies of k-step it have landed
-            __syncthreads();               // everyone's have; and stage (it - 1) % GSTAGES is free
-            if (it + GSTAGES - 1 < nk) issue(it + GSTAGES - 1);
-            cp_async_commit();
-            Stage& S = stg[it % GSTAGES];
+            Stage& S = stg[f % GSTAGES];
             if constexpr (SPLIT) {
                 // one k16 step: A rows g, g + 8 of each 16-row tile; k = 2 lc (+1), 2 lc + 8 (+1)
                 unsigned ah[2][4], am[2][4], al[2][4], bh[2][2], bm[2][2], bl[2][2];
@@ -297,7 +325,6 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
                 }
             }
         }
-        cp_async_wait<0>();
         if constexpr (SPLIT) {
 #pragma unroll
             for (int i = 0; i < 2; i++)
@@ -330,6 +357,7 @@ __device__ __noinline__ void team_gemm_t(const Team& t, bool ta, bool tb, int M,
             }
         }
     }
+    cp_async_wait<0>();
     __syncthreads();  // the stages are free for the next user
 }
 
