@@ -16,8 +16,8 @@
 //            (a reflector on rows j+1+s BW .. j+(s+1) BW) and applies it to the diagonal block
 //            and the block below. Sweep j+1 runs three steps behind sweep j (the tasks at one
 //            time step touch disjoint elements), one warp per sweep, the band (and its bulge, 2 BW
-//            diagonals) in global memory with each task's 32 x 32 blocks in the warp's shared
-//            tile;
+//            diagonals) in global memory by rows with each task's 32 x 32 blocks in the warp's
+//            shared tile;
 //   back     Z <- Q2 Z, then Z <- Q1 Z: the stage-2 reflectors of 32 consecutive sweeps at one
 //            step form a 64 x 64 orthogonal block (explicit, applied as a GEMM to 64 rows of Z;
 //            groups from the last, steps in ascending order, which respects every overlap), then
@@ -197,8 +197,9 @@ __device__ void team_sy2sb(const Team& t, double* A, long long lda, int n, doubl
 }
 
 // ---------------------------------------------------------------------------------- stage 2
-// band element (r, c) of the lower band storage (r >= c, r - c < LDB)
-__device__ __forceinline__ double* band_at(double* bd, int r, int c) { return bd + (long long)c * LDB + (r - c); }
+// band element (r, c) of the lower band storage (r >= c, r - c < LDB), stored by rows: a warp
+// whose lanes take consecutive columns of one row reads and writes consecutive addresses
+__device__ __forceinline__ double* band_at(double* bd, int r, int c) { return bd + (long long)r * LDB + (r - c); }
 
 // One bulge-chasing task (sweep j, step s) by one warp with its tile Tl (32 x 33) and vector
 // slots vs, ws (32 each). The tile holds, between steps of a sweep, the block below the previous
@@ -248,6 +249,7 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
     __syncwarp();
     // the diagonal block lo..hi, two-sided: y = tau D v, w = y - tau/2 (v.y) v, D -= v w^T + w v^T
     // (loads in batches of 16 independent ones per lane)
+    // the lower triangle by rows (coalesced), then mirrored in the tile
     if (lane < L) {
 #pragma unroll
         for (int r0 = 0; r0 < BW; r0 += 16) {
@@ -255,12 +257,16 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
 #pragma unroll
             for (int u = 0; u < 16; u++) {
                 int r = r0 + u;
-                tv[u] = r < L ? (r >= lane ? *band_at(bd, lo + r, lo + lane) : *band_at(bd, lo + lane, lo + r)) : 0.0;
+                tv[u] = (r < L && r >= lane) ? *band_at(bd, lo + r, lo + lane) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 16; u++) Tl[r0 + u][lane] = tv[u];
+            for (int u = 0; u < 16; u++)
+                if (r0 + u >= lane) Tl[r0 + u][lane] = tv[u];
         }
     }
+    __syncwarp();
+    if (lane < L)
+        for (int c = lane + 1; c < L; c++) Tl[lane][c] = Tl[c][lane];
     __syncwarp();
     if (tc != 0.0) {
         double y = 0.0;
@@ -272,9 +278,9 @@ __device__ void warp_chase(double* bd, int n, int j, int s, double (*Tl)[BW + 1]
         __syncwarp();
         if (lane < L) {
             double wl = ws[lane];
-            for (int r = lane; r < L; r++) {
+            for (int r = 0; r < L; r++) {  // row by row: the lanes write consecutive addresses
                 double d = Tl[r][lane] - (vs[r] * wl + ws[r] * v);
-                *band_at(bd, lo + r, lo + lane) = d;
+                if (r >= lane) *band_at(bd, lo + r, lo + lane) = d;
             }
         }
         __syncwarp();
@@ -312,8 +318,9 @@ __device__ void team_sb2st(const Team& t, const double* A, long long lda, int n,
     __shared__ double s_v[BWARPS][BW], s_w[BWARPS][BW];
     double* bd = wk + band_off_band(n);
     for (long long q = threadIdx.x; q < (long long)LDB * n; q += blockDim.x) {
-        int c = (int)(q / LDB), dg = (int)(q % LDB);
-        bd[q] = (dg <= BW && c + dg < n) ? A[c + dg + (long long)c * lda] : 0.0;
+        int dg = (int)(q % LDB);
+        int r = (int)(q / LDB);  // row r, diagonal dg: element (r, r - dg)
+        bd[q] = (dg <= BW && r - dg >= 0) ? A[r + (long long)(r - dg) * lda] : 0.0;
     }
     __syncthreads();
     int warp = threadIdx.x >> 5;
@@ -335,8 +342,8 @@ __device__ void team_sb2st(const Team& t, const double* A, long long lda, int n,
         }
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        d[i] = bd[(long long)i * LDB];
-        e[i] = i + 1 < n ? bd[(long long)i * LDB + 1] : 0.0;
+        d[i] = *band_at(bd, i, i);
+        e[i] = i + 1 < n ? *band_at(bd, i + 1, i) : 0.0;
     }
     __syncthreads();
 }
