@@ -78,11 +78,15 @@ __host__ __device__ __forceinline__ long long band_refl_index(int n, int j, int 
 // ---------------------------------------------------------------------------------- stage 1
 // Householder QR of the m x nb panel P (leading dimension ld) with nr reflectors: reflector c
 // acts on rows c..m-1, v_c = 1 at row c, kept below it in P; R above and on the diagonal; tau[c].
-// Warp w updates the columns q = w (mod 8); the warp owning column c + 1 also forms its norm
-// for the next reflector. Two CTA barriers per column.
+// Each reflector is also staged in shared memory; warp w updates the columns q = w (mod 8), all
+// of them in one pass over the rows (their dot products together, then their updates), and the
+// warp owning column c + 1 also forms its norm for the next reflector. Two CTA barriers per
+// column.
 __device__ void cta_panel_qr(double* P, long long ld, int m, int nb, int nr, double* tau) {
     __shared__ double s_xn2, s_alpha;
+    double* sv = s_work;  // the current reflector (m values)
     int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int QW = (BW + BWARPS - 1) / BWARPS;  // columns per warp
     if (warp == 0) {
         double xs = 0.0;
         for (int i = 1 + lane; i < m; i += 32) xs += sq(P[i]);
@@ -105,32 +109,61 @@ __device__ void cta_panel_qr(double* P, long long ld, int m, int nb, int nr, dou
             tc = (beta - alpha) / beta;
             scale = 1.0 / (alpha - beta);
         }
-        for (int i = c + 1 + threadIdx.x; i < m; i += blockDim.x) pc[i] *= scale;
+        for (int i = c + 1 + threadIdx.x; i < m; i += blockDim.x) {
+            double v = pc[i] * scale;
+            pc[i] = v;
+            sv[i] = v;
+        }
         __syncthreads();  // v visible; every thread has read s_xn2 and s_alpha
         if (threadIdx.x == 0) {
             pc[c] = beta;
             tau[c] = tc;
         }
-        for (int q = c + 1 + ((warp - (c + 1)) % BWARPS + BWARPS) % BWARPS; q < nb; q += BWARPS) {
-            double* pq = P + (long long)q * ld;
-            double w = 0.0;
-            for (int i = c + 1 + lane; i < m; i += 32) w = fma(pc[i], pq[i], w);
-            w = warp_sum(w) + pq[c];
-            double tw = tc * w;
-            __syncwarp();  // every lane has read pq[c]
-            if (lane == 0) pq[c] -= tw;
-            double xs = 0.0;
+        int q0 = c + 1 + ((warp - (c + 1)) % BWARPS + BWARPS) % BWARPS;
+        double* pq[QW];
+        bool on[QW];
+        double w[QW];
+#pragma unroll
+        for (int u = 0; u < QW; u++) {
+            int q = q0 + u * BWARPS;
+            on[u] = q < nb;
+            pq[u] = P + (long long)(on[u] ? q : c) * ld;
+            w[u] = 0.0;
+        }
+        if (q0 < nb) {  // uniform over the warp
+#pragma unroll 4
             for (int i = c + 1 + lane; i < m; i += 32) {
-                double x = pq[i] - tw * pc[i];
-                pq[i] = x;
-                if (i > c + 1) xs += x * x;
+                double vi = sv[i];
+#pragma unroll
+                for (int u = 0; u < QW; u++)
+                    if (on[u]) w[u] = fma(vi, pq[u][i], w[u]);
             }
-            if (q == c + 1) {
+            double tw[QW];
+#pragma unroll
+            for (int u = 0; u < QW; u++) tw[u] = on[u] ? tc * (warp_sum(w[u]) + pq[u][c]) : 0.0;
+            __syncwarp();  // every lane has read the pq[u][c]
+            if (lane == 0)
+#pragma unroll
+                for (int u = 0; u < QW; u++)
+                    if (on[u]) pq[u][c] -= tw[u];
+            double xs = 0.0;  // the norm below row c + 1 of column c + 1 (owned by u = 0 when q0 = c + 1)
+#pragma unroll 4
+            for (int i = c + 1 + lane; i < m; i += 32) {
+                double vi = sv[i];
+#pragma unroll
+                for (int u = 0; u < QW; u++)
+                    if (on[u]) {
+                        double x = pq[u][i] - tw[u] * vi;
+                        pq[u][i] = x;
+                        if (u == 0 && i > c + 1) xs += x * x;
+                    }
+            }
+            if (q0 == c + 1) {
                 xs = warp_sum(xs);
                 __syncwarp();
                 if (lane == 0) {
                     s_xn2 = xs;
-                    s_alpha = pq[c + 1];
+                    s_alpha = pq[0][c + 1];
                 }
             }
         }

@@ -1078,11 +1078,14 @@ __device__ __forceinline__ double hash_uniform(unsigned int a, unsigned int b) {
 // from bisection to working precision the first solve already amplifies the wanted direction by
 // ~1/eps, the second one settles it (LAPACK's dstein stops at that growth and adds one solve).
 // Vector q is written to column q of V (n x k, ldv). Work planes
-// u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved).
+// u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved); u0 keeps
+// the reciprocal pivots. The solves carry the running values in registers, so the loads of a
+// step (factors and right-hand side) do not wait for the previous step's stores.
 // Returns (through flag) nonzero when a vector was not finite.
 __device__ __noinline__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
-                           double* V, long long ldv, double* u0, double* u1, double* lm, unsigned char* piv, double* x,
-                           int* flag) {
+                                        double* V, long long ldv, double* __restrict__ u0, double* __restrict__ u1,
+                                        double* __restrict__ lm, unsigned char* __restrict__ piv,
+                                        double* __restrict__ x, int* flag) {
     double tnrm = 0.0;
     for (int i = 0; i < n; i++) {
         double r = fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
@@ -1106,10 +1109,10 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                 double sub = e[i], a1 = d[i + 1] - lam, b1 = (i + 2 < n) ? e[i + 1] : 0.0;
                 long long ix = (long long)i * LD + q;
                 if (fabs(ca) >= fabs(sub)) {
-                    double p = ca;
-                    if (p == 0.0) p = pivmin;
-                    double l = sub / p;
-                    u0[ix] = p;
+                    double pv = ca;
+                    if (pv == 0.0) pv = pivmin;
+                    double l = sub / pv;
+                    u0[ix] = 1.0 / pv;
                     u1[ix] = cb;
                     lm[ix] = l;
                     piv[ix] = 0;
@@ -1117,7 +1120,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                     cb = b1;
                 } else {
                     double l = ca / sub;
-                    u0[ix] = sub;
+                    u0[ix] = 1.0 / sub;
                     u1[ix] = a1;
                     lm[ix] = l;
                     piv[ix] = 1;
@@ -1127,52 +1130,53 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
             }
             {
                 long long ix = (long long)(n - 1) * LD + q;
-                u0[ix] = (ca == 0.0) ? pivmin : ca;
+                u0[ix] = 1.0 / ((ca == 0.0) ? pivmin : ca);
             }
             for (int i = 0; i < n; i++) x[(long long)i * LD + q] = hash_uniform((unsigned)q, (unsigned)i);
             for (int iter = 0; iter < 2; iter++) {
-                // forward: L with the row interchanges
+                // forward: L with the row interchanges; cur = row i after the earlier steps
+                double cur = x[q];
                 for (int i = 0; i + 1 < n; i++) {
                     long long ix = (long long)i * LD + q, ix1 = ix + LD;
-                    double xi = x[ix], xi1 = x[ix1];
+                    double nxt = x[ix1];
+                    double xi = cur, xi1 = nxt;
                     if (piv[ix]) {
-                        double tmp = xi;
-                        xi = xi1;
-                        xi1 = tmp;
-                        x[ix] = xi;
+                        xi = nxt;
+                        xi1 = cur;
                     }
-                    x[ix1] = xi1 - lm[ix] * xi;
+                    x[ix] = xi;
+                    cur = xi1 - lm[ix] * xi;
                 }
+                x[(long long)(n - 1) * LD + q] = cur;
                 // backward: U with up to two superdiagonals (u2_i = e_{i+1} after an interchange)
-                double xn1 = 0.0, xn2 = 0.0;
+                double xn1 = 0.0, xn2 = 0.0, mx = 0.0;
                 for (int i = n - 1; i >= 0; i--) {
                     long long ix = (long long)i * LD + q;
                     double v = x[ix];
                     if (i + 1 < n) v -= u1[ix] * xn1;
                     if (i + 2 < n && piv[ix]) v -= e[i + 1] * xn2;
-                    v /= u0[ix];
+                    v *= u0[ix];
                     x[ix] = v;
                     xn2 = xn1;
                     xn1 = v;
+                    mx = fmax(mx, fabs(v));
                 }
                 // scale by the largest element, orthogonalise within the cluster, normalise
-                double mx = 0.0;
-                for (int i = 0; i < n; i++) mx = fmax(mx, fabs(x[(long long)i * LD + q]));
                 if (!(mx > 0.0) || !isfinite(mx)) {
                     atomicOr(flag, ST_INVIT);
                     mx = 1.0;
                 }
                 double inv = 1.0 / mx;
                 for (int i = 0; i < n; i++) x[(long long)i * LD + q] *= inv;
-                for (int p = q0; p < q; p++) {
+                for (int pp = q0; pp < q; pp++) {
                     double dt = 0.0;
-                    for (int i = 0; i < n; i++) dt += x[(long long)i * LD + p] * x[(long long)i * LD + q];
-                    for (int i = 0; i < n; i++) x[(long long)i * LD + q] -= dt * x[(long long)i * LD + p];
+                    for (int i = 0; i < n; i++) dt += x[(long long)i * LD + pp] * x[(long long)i * LD + q];
+                    for (int i = 0; i < n; i++) x[(long long)i * LD + q] -= dt * x[(long long)i * LD + pp];
                 }
                 double nr = 0.0;
                 for (int i = 0; i < n; i++) nr += sq(x[(long long)i * LD + q]);
                 nr = 1.0 / sqrt(nr);
-                for (int i = 0; i < n; i++) x[(long long)i * LD + q] *= nr;
+                for (int i = 0; i < n; i++) x[(long long)i * LD + q] *= nr;  // later cluster members use it
             }
             for (int i = 0; i < n; i++) V[i + (long long)q * ldv] = x[(long long)i * LD + q];
         }
