@@ -29,7 +29,7 @@ class AxtbOptions(C.Structure):
                 ("guess", C.c_int32), ("precision", C.c_int32), ("device", C.c_int32), ("mixer", C.c_int32),
                 ("conventions", C.c_int32), ("solvation", C.c_int32), ("solvent", C.c_char_p),
                 ("solvation_state", C.c_int32), ("dispersion", C.c_int32),
-                ("band_min_nao", C.c_int32), ("grid_min_nao", C.c_int32)]
+                ("band_max_nao", C.c_int32), ("grid_min_nao", C.c_int32)]
 
 
 class AxtbResult(C.Structure):

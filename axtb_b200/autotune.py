@@ -4,13 +4,16 @@ on the whole GPU.
 The engine's eigen phase has two schedule choices, both exact (the results agree to
 round-off): the tridiagonal reduction of a one-CTA molecule (two-stage: band reduction on
 GEMMs, then bulge chasing; or one-stage Householder with the trailing matrix streamed per
-column), chosen by the size ``band_min_nao`` from which the two-stage one is used; and the size
+column), chosen by the size ``band_max_nao`` below which the two-stage one is used (measured on
+B200: it wins only for small molecules, where the one-stage reduction's per-column chain is
+short of work, not for large ones, where its bulge chasing waits on one global-memory round per
+block); and the size
 ``grid_min_nao`` from which a molecule's dense algebra runs on the whole cooperative grid
 instead of one CTA. The best crossovers depend on the GPU and the batch, so they are measured:
 
-* ``band_min_nao``: one profiled run of a sample batch with each reduction; the engine's
+* ``band_max_nao``: one profiled run of a sample batch with each reduction; the engine's
   per-molecule cycle counters of the eigen phase are binned by AO count, and the crossover is
-  the smallest bin from which the two-stage reduction is cheaper in every larger bin;
+  the largest bin edge below which the two-stage reduction is cheaper in every bin;
 * ``grid_min_nao``: whole runs of the sample with each candidate threshold below its largest
   molecule, timed with CUDA events; the fastest wins (no candidate applies to a sample without
   molecules that large, and the default stays).
@@ -26,7 +29,7 @@ from pathlib import Path
 
 import numpy as np
 
-DEFAULT = {"band_min_nao": 0, "grid_min_nao": 1024}
+DEFAULT = {"band_max_nao": 64, "grid_min_nao": 1024}
 GRID_CANDIDATES = (512, 768, 1024, 1536, 2048)
 
 
@@ -43,7 +46,7 @@ def _device_key(device: int) -> str:
 
 
 def schedule(device: int = 0) -> dict:
-    """The tuned options of this GPU (band_min_nao, grid_min_nao), or the defaults."""
+    """The tuned options of this GPU (band_max_nao, grid_min_nao), or the defaults."""
     try:
         data = json.loads(_cache_path().read_text())
         return dict(data[_device_key(device)]["options"])
@@ -52,22 +55,20 @@ def schedule(device: int = 0) -> dict:
 
 
 def crossover(nao: np.ndarray, cyc_two: np.ndarray, cyc_one: np.ndarray, width: int = 32) -> tuple[int, list]:
-    """The smallest AO count from which the two-stage reduction is cheaper in every bin of
-    `width` AOs (mean cycles per molecule of each bin), and the bins (lo, hi, n, two, one)."""
+    """The largest AO count below which the two-stage reduction is cheaper in every bin of `width`
+    AOs (mean cycles per molecule of each bin), and the bins (lo, hi, n, two, one)."""
     nao = np.asarray(nao)
     lo = (nao // width) * width
     bins = []
     for b in sorted(set(lo.tolist())):
         sel = lo == b
         bins.append((int(b), int(b + width), int(sel.sum()), float(np.mean(cyc_two[sel])), float(np.mean(cyc_one[sel]))))
-    cut = None
-    for b in reversed(bins):
+    cut = 0
+    for b in bins:
         if b[3] <= b[4]:
-            cut = b[0]
+            cut = b[1]
         else:
             break
-    if cut is None:
-        cut = bins[-1][1] if bins else DEFAULT["band_min_nao"]
     return int(cut), bins
 
 
@@ -121,21 +122,21 @@ def tune(molecules=None, device: int = 0, accuracy: float = 0.1, save: bool = Tr
     small = [m for m, n in zip(mols, nao) if n < grid]
     nsmall = np.array([n for n in nao if n < grid])
     opts = {"accuracy": accuracy, "grid_min_nao": grid}
-    band = DEFAULT["band_min_nao"]
+    band = DEFAULT["band_max_nao"]
     bins = []
     if small:
-        two = _eigen_cycles(small, dict(opts, band_min_nao=0), device)
-        one = _eigen_cycles(small, dict(opts, band_min_nao=1 << 30), device)
+        two = _eigen_cycles(small, dict(opts, band_max_nao=1 << 30), device)
+        one = _eigen_cycles(small, dict(opts, band_max_nao=0), device)
         band, bins = crossover(nsmall, two, one)
     grid_times = {}
     cands = [g for g in GRID_CANDIDATES if g <= int(nao.max())]
     if cands:
         for g in cands + [1 << 30]:
-            grid_times[g] = _timed_run(mols, {"accuracy": accuracy, "band_min_nao": band, "grid_min_nao": g}, device)
+            grid_times[g] = _timed_run(mols, {"accuracy": accuracy, "band_max_nao": band, "grid_min_nao": g}, device)
         grid = min(grid_times, key=grid_times.get)
         if grid == 1 << 30:
             grid = max(int(nao.max()) + 1, DEFAULT["grid_min_nao"])
-    result = {"options": {"band_min_nao": int(band), "grid_min_nao": int(grid)}, "bins": bins,
+    result = {"options": {"band_max_nao": int(band), "grid_min_nao": int(grid)}, "bins": bins,
               "grid_times": {str(k): v for k, v in grid_times.items()}, "sample": len(mols)}
     if save:
         path = _cache_path()

@@ -181,7 +181,7 @@ def _solvation(spec):
 
 
 def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", precision="fp64", device=0,
-             mixer=None, conventions="axtb", solvation=None, dispersion=True, band_min_nao=None,
+             mixer=None, conventions="axtb", solvation=None, dispersion=True, band_max_nao=None,
              grid_min_nao=None):
     model, solvent, state = _solvation(solvation)
     return _lib.default_options(accuracy=float(accuracy), etemp=float(etemp), max_iter=int(max_iter),
@@ -189,7 +189,7 @@ def _options(accuracy=1.0, etemp=300.0, max_iter=250, damping=0.4, guess="eeq", 
                                 precision={"fp64": 0, "split": 1}[precision], device=int(device),
                                 mixer=_mixer(mixer), conventions=_conventions(conventions), solvation=model,
                                 solvent=solvent, solvation_state=state, dispersion=1 if dispersion else 0,
-                                band_min_nao=-1 if band_min_nao is None else int(band_min_nao),
+                                band_max_nao=-1 if band_max_nao is None else int(band_max_nao),
                                 grid_min_nao=-1 if grid_min_nao is None else int(grid_min_nao))
 
 

@@ -240,12 +240,12 @@ struct Opt {
     std::string solvent;  // its solvent (xtb's names and aliases)
     int solv_state = 0;   // reference state: 0 gsolv, 1 bar1M, 2 reference
     int dispersion = 1;   // 0: leave the D4 term out (crates/axtb/src/lib.rs:107, 185-187)
-    int band_min_nao = -1;  // schedule: two-stage reduction from this many AOs (-1: default)
+    int band_max_nao = -1;  // schedule: two-stage reduction below this many AOs (-1: default)
     int grid_min_nao = -1;  // schedule: whole-grid teams from this many AOs (-1: default)
 };
 
 // default schedule of the dense algebra (axtb_b200.autotune measures both crossovers on a device)
-constexpr int DEFAULT_BAND_MIN_NAO = 0;
+constexpr int DEFAULT_BAND_MAX_NAO = 64;
 constexpr int DEFAULT_GRID_MIN_NAO = 1024;
 
 // ------------------------------------------------------------------ solvation parameters
@@ -863,10 +863,10 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.max_iter = o.max_iter;
     b.split = o.precision == 1 ? 1 : 0;
     b.disp = o.dispersion ? 1 : 0;
-    // one-CTA molecules from band_min_nao AOs on reduce to tridiagonal form in two stages, the
-    // smaller ones (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
-    b.band_min = o.band_min_nao >= 0 ? o.band_min_nao : DEFAULT_BAND_MIN_NAO;
-    if (std::getenv("AXTB_EIGEN_ONESTAGE")) b.band_min = 1 << 30;
+    // one-CTA molecules below band_max_nao AOs reduce to tridiagonal form in two stages, the
+    // larger ones (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
+    b.band_max = o.band_max_nao >= 0 ? o.band_max_nao : DEFAULT_BAND_MAX_NAO;
+    if (std::getenv("AXTB_EIGEN_ONESTAGE")) b.band_max = 0;
     // state
     axg::State& s = S;
     s.xyz = ar.take<double>(natT * 3);
@@ -1514,7 +1514,7 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.P = d_density;
     B.nmol = 1;
     B.kt = kt;
-    B.band_min = 0;
+    B.band_max = DEFAULT_BAND_MAX_NAO;
     axg::k_density_static<<<1, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta,
                                                                                               d_status);
     cudaError_t e = cudaGetLastError();

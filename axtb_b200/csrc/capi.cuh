@@ -187,7 +187,7 @@ static Opt to_opt(const AxtbOptions* o) {
         r.solvent = o->solvent ? o->solvent : "";
         r.solv_state = o->solvation_state;
         r.dispersion = o->dispersion != 0 ? 1 : 0;
-        r.band_min_nao = o->band_min_nao;
+        r.band_max_nao = o->band_max_nao;
         r.grid_min_nao = o->grid_min_nao;
     }
     return r;
@@ -238,7 +238,7 @@ void axtb_gpu_default_options(AxtbOptions* o) {
     o->solvent = nullptr;
     o->solvation_state = 0;
     o->dispersion = 1;
-    o->band_min_nao = -1;
+    o->band_max_nao = -1;
     o->grid_min_nao = -1;
 }
 

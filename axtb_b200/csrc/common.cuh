@@ -81,7 +81,7 @@ struct Batch {
     const double* sv_srcut;
     int split;                        // 1: basis-transform and W GEMMs in split precision
     int disp;                         // 0: the D4 term is left out (Options::dispersion = false)
-    int band_min;                     // one-CTA molecules from this many AOs reduce to tridiagonal form in two stages
+    int band_max;                     // one-CTA molecules below this many AOs reduce to tridiagonal form in two stages
 };
 
 // per-geometry and per-iteration device state

@@ -163,7 +163,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
     const int nsl = symv_slots(n);
-    const bool band = !t.global && n >= B.band_min;
+    const bool band = !t.global && n < B.band_max;
     if (band) {
         // one CTA: two-stage reduction (dense -> band on GEMMs, band -> tridiagonal by bulge
         // chasing), the stage-2 reflectors in the W plane (free until the gradient's W)
@@ -185,9 +185,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     // filling is redone, so every level with f > 1e-16 is a true eigenvalue.
     team_gershgorin(t, d, e, n, wk);
     int kc = min(n, (int)ceil(fmax(B.m_nalpha[m], B.m_nbeta[m])) + max(16, n / 16));
-    // after the first iteration of an attempt, the previous iteration's levels (still in emo)
-    // give narrow starting brackets (checked by Sturm counts; the same run gives the same bits)
-    team_bisect(t, d, e, n, emo, wk, 0, kc, S.iter[m] > 0);
+    team_bisect(t, d, e, n, emo, wk, 0, kc);
     for (int q = kc + t.tid(); q < n; q += t.nthreads()) emo[q] = wk[1];
     t.sync();
     TEAM_PHASE(2);

@@ -858,13 +858,9 @@ __device__ __forceinline__ bool bisect_done(double lo, double hi, double pivmin)
 }
 
 // R eigenvalues per thread (k = k0 + threadIdx.x + r blockDim.x), bisection interleaved
-// The bracket of eigenvalue k from its value wk of the previous SCF iteration: wk +- delta when
-// the Sturm counts confirm that it holds the k-th eigenvalue, else the Gershgorin interval
-constexpr double BISECT_WARM = 1e-4;
-
 template <int R>
 __device__ void cta_bisect_ilp(const double* sd, const double* se2, int n, double* w, double glo, double ghi,
-                               double pivmin, int k0, int k1, bool warm) {
+                               double pivmin, int k0, int k1) {
     double lo[R], hi[R], x[R];
     int cnt[R];
     bool live[R];
@@ -873,27 +869,6 @@ __device__ void cta_bisect_ilp(const double* sd, const double* se2, int n, doubl
         lo[r] = glo;
         hi[r] = ghi;
         live[r] = k0 + (int)threadIdx.x + r * (int)blockDim.x < k1;
-    }
-    if (warm) {
-        double xl[R], xh[R];
-        int cl[R], ch[R];
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            int k = k0 + (int)threadIdx.x + r * (int)blockDim.x;
-            double wk = live[r] ? w[k] : 0.0, dl = BISECT_WARM * fmax(1.0, fabs(wk));
-            xl[r] = wk - dl;
-            xh[r] = wk + dl;
-        }
-        sturm_counts_sh<R>(sd, se2, n, xl, pivmin, cl);
-        sturm_counts_sh<R>(sd, se2, n, xh, pivmin, ch);
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            int k = k0 + (int)threadIdx.x + r * (int)blockDim.x;
-            if (live[r] && cl[r] <= k && ch[r] > k && xl[r] > glo && xh[r] < ghi) {
-                lo[r] = xl[r];
-                hi[r] = xh[r];
-            }
-        }
     }
     for (int it = 0; it < 200; it++) {
         bool any = false;
@@ -925,22 +900,12 @@ __device__ void cta_bisect_ilp(const double* sd, const double* se2, int n, doubl
 // evaluate the Sturm count at g interior points of the bracket, which shrinks to the (g+1)-th
 // part holding the eigenvalue (log2(g+1) bits per step instead of one)
 __device__ void cta_bisect_groups(const double* sd, const double* se2, int n, double* w, double glo, double ghi,
-                                  double pivmin, int k0, int k1, int g, bool warm) {
+                                  double pivmin, int k0, int k1, int g) {
     int lane = threadIdx.x & 31, gl = lane % g, base = lane - gl;
     unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << base);
     int k = k0 + (int)threadIdx.x / g;
     bool live = k < k1;
     double lo = glo, hi = ghi;
-    if (warm && live) {  // every lane of the group makes the same test
-        double wk = w[k], dl = BISECT_WARM * fmax(1.0, fabs(wk));
-        double xb[2] = {wk - dl, wk + dl};
-        int cb[2];
-        sturm_counts_sh<2>(sd, se2, n, xb, pivmin, cb);
-        if (cb[0] <= k && cb[1] > k && xb[0] > glo && xb[1] < ghi) {
-            lo = xb[0];
-            hi = xb[1];
-        }
-    }
     for (int it = 0; it < 200; it++) {
         double h = (hi - lo) / (double)(g + 1);
         double xf = lo + h, xl = lo + (double)g * h;
@@ -962,8 +927,7 @@ __device__ void cta_bisect_groups(const double* sd, const double* se2, int n, do
 }
 
 // eigenvalues k0..k1-1 of one CTA's tridiagonal (d, e), d and e^2 staged in shared memory
-__device__ void cta_bisect(const double* d, const double* e, int n, double* w, const double* gbuf, int k0, int k1,
-                           bool warm) {
+__device__ void cta_bisect(const double* d, const double* e, int n, double* w, const double* gbuf, int k0, int k1) {
     double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
     double* sd = s_work;
     double* se2 = s_work + n;
@@ -978,27 +942,26 @@ __device__ void cta_bisect(const double* d, const double* e, int n, double* w, c
         if (cnt <= nt / 2) {
             int g = 2;
             while (g < 32 && nt / (2 * g) >= cnt) g *= 2;
-            cta_bisect_groups(sd, se2, n, w, glo, ghi, pivmin, k0, k1, g, warm);
+            cta_bisect_groups(sd, se2, n, w, glo, ghi, pivmin, k0, k1, g);
         } else if (cnt <= nt) {
-            cta_bisect_ilp<1>(sd, se2, n, w, glo, ghi, pivmin, k0, k1, warm);
+            cta_bisect_ilp<1>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
         } else if (cnt <= 2 * nt) {
-            cta_bisect_ilp<2>(sd, se2, n, w, glo, ghi, pivmin, k0, k1, warm);
+            cta_bisect_ilp<2>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
         } else if (cnt <= 3 * nt) {
-            cta_bisect_ilp<3>(sd, se2, n, w, glo, ghi, pivmin, k0, k1, warm);
+            cta_bisect_ilp<3>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
         } else {
-            cta_bisect_ilp<4>(sd, se2, n, w, glo, ghi, pivmin, k0, k1, warm);
+            cta_bisect_ilp<4>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
         }
     }
     __syncthreads();
 }
 
 // eigenvalues k0..k1-1 (ascending order) by bisection, one thread per eigenvalue index; gbuf holds
-// team_gershgorin's bounds. One CTA whose matrix fits the shared work area: cta_bisect, which with
-// `warm` starts from narrow brackets around the values w holds (the previous SCF iteration's).
+// team_gershgorin's bounds. One CTA whose matrix fits the shared work area: cta_bisect.
 __device__ __noinline__ void team_bisect(const Team& t, const double* d, const double* e, int n, double* w,
-                                         const double* gbuf, int k0, int k1, bool warm = false) {
+                                         const double* gbuf, int k0, int k1) {
     if (!t.global && 2 * n <= SMEM_WORK && k1 - k0 <= 4 * (int)blockDim.x) {
-        cta_bisect(d, e, n, w, gbuf, k0, k1, warm);
+        cta_bisect(d, e, n, w, gbuf, k0, k1);
         return;
     }
     double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];

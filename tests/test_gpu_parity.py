@@ -184,9 +184,9 @@ def test_autotuned_schedule_gives_the_same_results(engine, tmp_path, monkeypatch
     res = autotune.tune(mols, accuracy=1e-6)
     opts = res["options"]
     assert opts == autotune.schedule()
-    assert 0 <= opts["band_min_nao"] and opts["grid_min_nao"] >= 512
+    assert 0 <= opts["band_max_nao"] and opts["grid_min_nao"] >= 512
     base = engine.Batch(mols, accuracy=1e-6).run(gradient=True)
-    for sched in (opts, {"band_min_nao": 1 << 30}, {"band_min_nao": 0, "grid_min_nao": 200}):
+    for sched in (opts, {"band_max_nao": 0}, {"band_max_nao": 1 << 30, "grid_min_nao": 200}):
         other = engine.Batch(mols, accuracy=1e-6, **sched).run(gradient=True)
         for a, b in zip(base, other):
             assert a.status == b.status == 0
