@@ -1041,9 +1041,9 @@ __device__ __forceinline__ double hash_uniform(unsigned int a, unsigned int b) {
 // from bisection to working precision the first solve already amplifies the wanted direction by
 // ~1/eps, the second one settles it (LAPACK's dstein stops at that growth and adds one solve).
 // Vector q is written to column q of V (n x k, ldv). Work planes
-// u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved); u0 keeps
-// the reciprocal pivots. The solves carry the running values in registers, so the loads of a
-// step (factors and right-hand side) do not wait for the previous step's stores.
+// u0, u1, lm (n*n each, interleaved [i*n + q]), piv (n*n bytes), x (n*n interleaved). The solves
+// carry the running values in registers, so the loads of a step (factors and right-hand side)
+// do not wait for the previous step's stores.
 // Returns (through flag) nonzero when a vector was not finite.
 __device__ __noinline__ void team_invit(const Team& t, const double* d, const double* e, const double* w, int n, int k,
                                         double* V, long long ldv, double* __restrict__ u0, double* __restrict__ u1,
@@ -1075,7 +1075,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                     double pv = ca;
                     if (pv == 0.0) pv = pivmin;
                     double l = sub / pv;
-                    u0[ix] = 1.0 / pv;
+                    u0[ix] = pv;
                     u1[ix] = cb;
                     lm[ix] = l;
                     piv[ix] = 0;
@@ -1083,7 +1083,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                     cb = b1;
                 } else {
                     double l = ca / sub;
-                    u0[ix] = 1.0 / sub;
+                    u0[ix] = sub;
                     u1[ix] = a1;
                     lm[ix] = l;
                     piv[ix] = 1;
@@ -1093,7 +1093,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
             }
             {
                 long long ix = (long long)(n - 1) * LD + q;
-                u0[ix] = 1.0 / ((ca == 0.0) ? pivmin : ca);
+                u0[ix] = (ca == 0.0) ? pivmin : ca;
             }
             for (int i = 0; i < n; i++) x[(long long)i * LD + q] = hash_uniform((unsigned)q, (unsigned)i);
             for (int iter = 0; iter < 2; iter++) {
@@ -1118,7 +1118,7 @@ __device__ __noinline__ void team_invit(const Team& t, const double* d, const do
                     double v = x[ix];
                     if (i + 1 < n) v -= u1[ix] * xn1;
                     if (i + 2 < n && piv[ix]) v -= e[i + 1] * xn2;
-                    v *= u0[ix];
+                    v /= u0[ix];
                     x[ix] = v;
                     xn2 = xn1;
                     xn1 = v;

@@ -41,8 +41,10 @@ def test_large_molecule_matches_oracle(engine, name):
     de = abs(r.energy - float(ref[f"{name}_energy"]))
     dg = float(np.abs(r.gradient - ref[f"{name}_gradient"]).max())
     dq = float(np.abs(r.charges - ref[f"{name}_qat"]).max())
+    names = ("repulsion", "dispersion", "electronic", "isotropic_es", "third_order", "anisotropic", "entropy", "band")
+    dterms = {k: float(r.terms[k] - t) for k, t in zip(names, ref[f"{name}_terms"])}
     print(f"{name}: {len(z)} atoms, {nao} AOs, |dE| = {de:.2e} Eh, max|dG| = {dg:.2e} Eh/bohr, max|dq| = {dq:.2e}, "
-          f"{r.iterations} iterations (oracle {int(ref[f'{name}_iterations'])})")
+          f"{r.iterations} iterations (oracle {int(ref[f'{name}_iterations'])}); term differences {dterms}")
     assert de < E_TOL
     assert dg < G_TOL
     assert dq < 1e-7
