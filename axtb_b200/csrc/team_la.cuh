@@ -896,36 +896,6 @@ __device__ void cta_bisect_ilp(const double* sd, const double* se2, int n, doubl
     }
 }
 
-// one eigenvalue per group of g lanes (g a power of two <= 32): each step the group's lanes
-// evaluate the Sturm count at g interior points of the bracket, which shrinks to the (g+1)-th
-// part holding the eigenvalue (log2(g+1) bits per step instead of one)
-__device__ void cta_bisect_groups(const double* sd, const double* se2, int n, double* w, double glo, double ghi,
-                                  double pivmin, int k0, int k1, int g) {
-    int lane = threadIdx.x & 31, gl = lane % g, base = lane - gl;
-    unsigned gmask = g == 32 ? 0xffffffffu : (((1u << g) - 1u) << base);
-    int k = k0 + (int)threadIdx.x / g;
-    bool live = k < k1;
-    double lo = glo, hi = ghi;
-    for (int it = 0; it < 200; it++) {
-        double h = (hi - lo) / (double)(g + 1);
-        double xf = lo + h, xl = lo + (double)g * h;
-        if (live && (bisect_done(lo, hi, pivmin) || !(xf > lo && xl < hi))) live = false;
-        if (!__any_sync(0xffffffffu, live)) break;
-        double x = lo + (double)(gl + 1) * h;
-        int c = 0;
-        if (live) sturm_counts_sh<1>(sd, se2, n, &x, pivmin, &c);
-        unsigned below = __ballot_sync(0xffffffffu, live && c <= k) & gmask;
-        int j = __popc(below);  // points at or below the eigenvalue: a prefix of the group
-        double xlo = __shfl_sync(0xffffffffu, x, base + max(j - 1, 0));
-        double xhi = __shfl_sync(0xffffffffu, x, base + min(j, g - 1));
-        if (live) {
-            if (j > 0) lo = xlo;
-            if (j < g) hi = xhi;
-        }
-    }
-    if (k < k1 && gl == 0) w[k] = 0.5 * (lo + hi);
-}
-
 // eigenvalues k0..k1-1 of one CTA's tridiagonal (d, e), d and e^2 staged in shared memory
 __device__ void cta_bisect(const double* d, const double* e, int n, double* w, const double* gbuf, int k0, int k1) {
     double glo = gbuf[0], ghi = gbuf[1], pivmin = gbuf[2];
@@ -939,11 +909,9 @@ __device__ void cta_bisect(const double* d, const double* e, int n, double* w, c
     __syncthreads();
     int cnt = k1 - k0, nt = blockDim.x;
     if (cnt > 0) {
-        if (cnt <= nt / 2) {
-            int g = 2;
-            while (g < 32 && nt / (2 * g) >= cnt) g *= 2;
-            cta_bisect_groups(sd, se2, n, w, glo, ghi, pivmin, k0, k1, g);
-        } else if (cnt <= nt) {
+        // plain bisection per level (multisection takes fewer steps for few levels, but ends on
+        // other bits, and a few chaotic SCFs follow those bits)
+        if (cnt <= nt) {
             cta_bisect_ilp<1>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);
         } else if (cnt <= 2 * nt) {
             cta_bisect_ilp<2>(sd, se2, n, w, glo, ghi, pivmin, k0, k1);

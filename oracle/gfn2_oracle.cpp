@@ -2618,8 +2618,13 @@ int run(OracleRun* R) {
             for (int a = 0; a < nsh; a++) e3 += out.qsh[a] * out.qsh[a] * out.qsh[a] * md.gam3[a] / 3.0;
             double eaes = aes_energy(md, ac, out.qat, out.dp, out.qp);
             double edisp = d4.off ? 0.0 : d4_energy(d4, out.qat, nullptr);
+            // band energy column by column, the columns' dots summed in order (xtb.rs:1130-1133)
             double band = 0.0;
-            for (size_t k = 0; k < (size_t)nao * nao; k++) band += I.H0[k] * P[k];
+            for (int nu = 0; nu < nao; nu++) {
+                double col = 0.0;
+                for (int mu = 0; mu < nao; mu++) col += I.H0[(size_t)mu + (size_t)nu * nao] * P[(size_t)mu + (size_t)nu * nao];
+                band += col;
+            }
             double esolv = solv ? solv_energy(sv, out.qat) : 0.0;
             esolv_last = esolv;
             double energy = e2 + e3 + eaes + edisp + ts + band + esolv;
