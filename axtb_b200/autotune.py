@@ -4,7 +4,8 @@ on the whole GPU.
 The engine's eigen phase has two schedule choices, both exact (the results agree to
 round-off): the tridiagonal reduction of a one-CTA molecule (two-stage: band reduction on
 GEMMs, then bulge chasing; or one-stage Householder with the trailing matrix streamed per
-column), chosen by the size ``band_max_nao`` below which the two-stage one is used (measured on
+column), chosen by the size ``band_max_nao`` below which the two-stage one is used (from 34 AOs:
+a smaller matrix already is a band, and keeps the one-stage reduction; measured on
 B200: it wins only for small molecules, where the one-stage reduction's per-column chain is
 short of work, not for large ones, where its bulge chasing waits on one global-memory round per
 block); and the size

@@ -863,8 +863,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.max_iter = o.max_iter;
     b.split = o.precision == 1 ? 1 : 0;
     b.disp = o.dispersion ? 1 : 0;
-    // one-CTA molecules below band_max_nao AOs reduce to tridiagonal form in two stages, the
-    // larger ones (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
+    // one-CTA molecules of 34 AOs up to below band_max_nao reduce to tridiagonal form in two
+    // stages, the others (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
     b.band_max = o.band_max_nao >= 0 ? o.band_max_nao : DEFAULT_BAND_MAX_NAO;
     if (std::getenv("AXTB_EIGEN_ONESTAGE")) b.band_max = 0;
     // state

@@ -163,7 +163,9 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
     const int nsl = symv_slots(n);
-    const bool band = !t.global && n < B.band_max;
+    // the two-stage path needs a band stage: a matrix of at most BW + 1 rows already is a band,
+    // and the one-stage path keeps the bits that small chaotic SCFs follow
+    const bool band = !t.global && n > BW + 1 && n < B.band_max;
     if (band) {
         // one CTA: two-stage reduction (dense -> band on GEMMs, band -> tridiagonal by bulge
         // chasing), the stage-2 reflectors in the W plane (free until the gradient's W)

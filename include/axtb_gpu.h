@@ -76,8 +76,8 @@ typedef struct AxtbOptions {
     int32_t dispersion;  /* 1 (default): with the D4 dispersion term; 0: without it (Options::dispersion,
                           crates/axtb/src/lib.rs:106-107, 185-187: for validation only) */
     int32_t band_max_nao; /* schedule of the dense algebra (no reference counterpart; results agree to
-                          round-off either way): molecules below this many AOs use the two-stage
-                          tridiagonal reduction, larger ones the one-stage one; -1 the default (64;
+                          round-off either way): molecules of 34 AOs up to below this many use the
+                          two-stage tridiagonal reduction, the others the one-stage one; -1 the default (64;
                           axtb_b200.autotune measures the crossover on a device) */
     int32_t grid_min_nao; /* molecules from this many AOs run their dense algebra on the whole GPU,
                           the rest one per CTA; -1 the default (1024) */
