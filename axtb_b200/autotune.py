@@ -13,8 +13,10 @@ block); and the size
 instead of one CTA. The best crossovers depend on the GPU and the batch, so they are measured:
 
 * ``band_max_nao``: one profiled run of a sample batch with each reduction; the engine's
-  per-molecule cycle counters of the eigen phase are binned by AO count, and the crossover is
-  the largest bin edge below which the two-stage reduction is cheaper in every bin;
+  per-molecule cycle counters of the eigen phase (the on-chip bulge chasing counted in units of
+  the team kernel's half-SM CTAs) are binned by AO count, and the bin edge that minimises the
+  sample's total with the two-stage reduction below it is the candidate; it, the default and 0
+  (one-stage only) are then timed as whole runs of the sample, and the fastest is kept;
 * ``grid_min_nao``: whole runs of the sample with each candidate threshold below its largest
   molecule, timed with CUDA events; the fastest wins (no candidate applies to a sample without
   molecules that large, and the default stays).
@@ -56,20 +58,22 @@ def schedule(device: int = 0) -> dict:
 
 
 def crossover(nao: np.ndarray, cyc_two: np.ndarray, cyc_one: np.ndarray, width: int = 32) -> tuple[int, list]:
-    """The largest AO count below which the two-stage reduction is cheaper in every bin of `width`
-    AOs (mean cycles per molecule of each bin), and the bins (lo, hi, n, two, one)."""
+    """The AO count below which the two-stage reduction is used: of the bin edges (bins of `width`
+    AOs), the one that minimises the sample's total eigen cycles with the two-stage reduction below
+    it and the one-stage reduction from it on (0 when no edge beats the one-stage reduction
+    everywhere); and the bins (lo, hi, n, mean two-stage cycles, mean one-stage cycles)."""
     nao = np.asarray(nao)
+    cyc_two, cyc_one = np.asarray(cyc_two, dtype=float), np.asarray(cyc_one, dtype=float)
     lo = (nao // width) * width
     bins = []
     for b in sorted(set(lo.tolist())):
         sel = lo == b
         bins.append((int(b), int(b + width), int(sel.sum()), float(np.mean(cyc_two[sel])), float(np.mean(cyc_one[sel]))))
-    cut = 0
-    for b in bins:
-        if b[3] <= b[4]:
-            cut = b[1]
-        else:
-            break
+    best, cut, run = 0.0, 0, 0.0
+    for b in bins:  # running sum of the saving (two - one) over the bins below each upper edge
+        run += b[2] * (b[3] - b[4])
+        if run < best:
+            best, cut = run, b[1]
     return int(cut), bins
 
 
@@ -125,10 +129,17 @@ def tune(molecules=None, device: int = 0, accuracy: float = 0.1, save: bool = Tr
     opts = {"accuracy": accuracy, "grid_min_nao": grid}
     band = DEFAULT["band_max_nao"]
     bins = []
+    band_times = {}
     if small:
         two = _eigen_cycles(small, dict(opts, band_max_nao=1 << 30), device)
         one = _eigen_cycles(small, dict(opts, band_max_nao=0), device)
-        band, bins = crossover(nsmall, two, one)
+        cut, bins = crossover(nsmall, two, one)
+        # the per-molecule cycles do not see the launches' tails (the two-stage eigen phase is
+        # three launches, each balanced on its own): the cut, the default and none are timed as
+        # whole runs of the sample, and the fastest wins
+        for bm in sorted({0, DEFAULT["band_max_nao"], cut}):
+            band_times[bm] = _timed_run(mols, {"accuracy": accuracy, "band_max_nao": bm, "grid_min_nao": grid}, device)
+        band = min(band_times, key=band_times.get)
     grid_times = {}
     cands = [g for g in GRID_CANDIDATES if g <= int(nao.max())]
     if cands:
@@ -138,6 +149,7 @@ def tune(molecules=None, device: int = 0, accuracy: float = 0.1, save: bool = Tr
         if grid == 1 << 30:
             grid = max(int(nao.max()) + 1, DEFAULT["grid_min_nao"])
     result = {"options": {"band_max_nao": int(band), "grid_min_nao": int(grid)}, "bins": bins,
+              "band_times": {str(k): v for k, v in band_times.items()},
               "grid_times": {str(k): v for k, v in grid_times.items()}, "sample": len(mols)}
     if save:
         path = _cache_path()

@@ -29,6 +29,7 @@
 #include "k_solvation.cuh"
 #include "params/gfn2_tables.h"
 #include "team_kernel.cuh"
+#include "chase.cuh"
 
 using std::vector;
 
@@ -244,8 +245,12 @@ struct Opt {
     int grid_min_nao = -1;  // schedule: whole-grid teams from this many AOs (-1: default)
 };
 
-// default schedule of the dense algebra (axtb_b200.autotune measures both crossovers on a device)
+// default schedule of the dense algebra (axtb_b200.autotune measures both crossovers on a device):
+// the two-stage reduction below 64 AOs (measured on B200: per molecule it is also cheaper between
+// 224 and 416 AOs with the bulge chasing on chip, but whole batches run no faster, the eigen phase
+// then being three launches with three tails)
 constexpr int DEFAULT_BAND_MAX_NAO = 64;
+constexpr int STATIC_BAND_MAX_NAO = 64;
 constexpr int DEFAULT_GRID_MIN_NAO = 1024;
 
 // ------------------------------------------------------------------ solvation parameters
@@ -324,6 +329,8 @@ struct AxtbBatch {
     axg::Batch B{};
     axg::State S{};
     axg::TeamPlan P{};
+    axg::ChasePlan CP{};    // molecules whose band k_chase reduces (stage 2 on chip)
+    int nchase = 0, chase_grid = 0;
     void* dmem = nullptr;
     void* hpin = nullptr;  // pinned staging
     size_t hpin_size = 0;
@@ -353,7 +360,7 @@ struct AxtbBatch {
         double ms = 0, flops = 0, bytes = 0;
     };
     bool profiling = false;
-    double team_cycles[16] = {0};
+    double team_cycles[axg::TEAM_CYCLE_SLOTS] = {0};
     std::vector<double> eigen_ms;  // each eigen launch of the last profiled run (ms)
     vector<Rec> recs;
     std::map<std::string, Acc> prof;
@@ -587,6 +594,25 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
             sp_rr[a * nsp + b] = v;
             sp_r0[a * nsp + b] = 0.52 * std::sqrt(v) + 5.0;
         }
+    // one-CTA molecules of 34 AOs up to below band_max_nao reduce to tridiagonal form in two
+    // stages, the others (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
+    int band_max = o.band_max_nao >= 0 ? o.band_max_nao : DEFAULT_BAND_MAX_NAO;
+    if (std::getenv("AXTB_EIGEN_ONESTAGE")) band_max = 0;
+    // stage 2 of those in shared memory (k_chase: one CTA per SM, a cluster pair above CHASE_ROWS
+    // AOs) when the device offers the shared memory and clusters (AXTB_STAGE2_IN_TEAM=1: in the
+    // team kernel, the band in global memory; the same results)
+    int chase_max = 0;
+    {
+        int optin = 0, clusters = 0;
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+        CK(cudaDeviceGetAttribute(&clusters, cudaDevAttrClusterLaunch, device));
+        if (optin >= axg::CHASE_DYN_BYTES + axg::CHASE_STATIC_BYTES && clusters &&
+            !std::getenv("AXTB_STAGE2_IN_TEAM")) {
+            CK(cudaFuncSetAttribute((const void*)axg::k_chase, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    axg::CHASE_DYN_BYTES));
+            chase_max = axg::CHASE_MAX_NAO;
+        }
+    }
     // ---- team plan: molecules from 1024 AOs on run on the whole grid, the rest one per CTA
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
@@ -595,31 +621,50 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, axg::k_team, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES));
     if (per <= 0) throw Fail(AXTB_ERR_DEVICE, "team kernel does not fit on a multiprocessor");
     grid = nsm * std::min(per, 2);
-    vector<int> big, small_off(grid + 1, 0), small_list;
+    vector<int> big, small_off(grid + 1, 0), small_list, head_off, head_list, tail_off, tail_list;
     {
-        vector<std::pair<double, int>> smalls;
+        vector<std::pair<double, int>> smalls, heads, tails;
         // molecules from this many AOs on take the whole grid (AXTB_TEAM_BIG_NAO overrides, e.g.
         // to run small molecules through the grid-wide path in tests)
         int big_nao = o.grid_min_nao > 0 ? o.grid_min_nao : DEFAULT_GRID_MIN_NAO;
         if (const char* e = std::getenv("AXTB_TEAM_BIG_NAO")) big_nao = std::max(1, std::atoi(e));
+        // the eigen phase of a molecule whose bulge chasing runs on chip is split over two team
+        // launches (before and after k_chase), each balanced on its own: measured shares of a
+        // two-stage eigen phase, ~0.2 before (F' and stage 1) and ~0.55 after
         for (int m = 0; m < nmol; m++) {
-            if (m_nao[m] >= big_nao) big.push_back(m);
-            else smalls.push_back({std::pow((double)m_nao[m] + 32.0, 3.0), m});
+            int n = m_nao[m];
+            if (n >= big_nao) {
+                big.push_back(m);
+                continue;
+            }
+            double c = std::pow((double)n + 32.0, 3.0);
+            bool chased = n > axg::BW + 1 && n < band_max && n <= chase_max;
+            smalls.push_back({c, m});
+            heads.push_back({chased ? 0.2 * c : c, m});
+            if (chased) tails.push_back({0.55 * c, m});
         }
-        std::sort(smalls.begin(), smalls.end(), [](auto& x, auto& y) { return x.first > y.first; });
-        vector<vector<int>> lists(grid);
-        std::priority_queue<std::pair<double, int>, vector<std::pair<double, int>>, std::greater<>> pq;
-        for (int g = 0; g < grid; g++) pq.push({0.0, g});
-        for (auto& s : smalls) {
-            auto top = pq.top();
-            pq.pop();
-            lists[top.second].push_back(s.second);
-            pq.push({top.first + s.first, top.second});
-        }
-        for (int g = 0; g < grid; g++) {
-            small_off[g + 1] = small_off[g] + (int)lists[g].size();
-            for (int m : lists[g]) small_list.push_back(m);
-        }
+        // longest first onto the least loaded CTA
+        auto lpt = [&](vector<std::pair<double, int>>& items, vector<int>& off, vector<int>& list) {
+            std::sort(items.begin(), items.end(), [](auto& x, auto& y) { return x.first > y.first; });
+            vector<vector<int>> lists(grid);
+            std::priority_queue<std::pair<double, int>, vector<std::pair<double, int>>, std::greater<>> pq;
+            for (int g = 0; g < grid; g++) pq.push({0.0, g});
+            for (auto& it : items) {
+                auto top = pq.top();
+                pq.pop();
+                lists[top.second].push_back(it.second);
+                pq.push({top.first + it.first, top.second});
+            }
+            off.assign(grid + 1, 0);
+            list.clear();
+            for (int g = 0; g < grid; g++) {
+                off[g + 1] = off[g] + (int)lists[g].size();
+                for (int m : lists[g]) list.push_back(m);
+            }
+        };
+        lpt(smalls, small_off, small_list);
+        lpt(heads, head_off, head_list);
+        lpt(tails, tail_off, tail_list);
     }
     // ---- device allocation (one arena)
     size_t bytes = 0;
@@ -638,6 +683,17 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     addI(nsp + nsp * 7);
     addD(nsp * 7 * 2 + nsp * 4 + (size_t)nsp * nsp * 49 + (size_t)nsp * nsp * 2);
     addI(big.size() + 1 + small_off.size() + small_list.size() + 1);
+    addI(head_off.size());  // the eigen phase's own plans (before and after k_chase)
+    addI(head_list.size() + 1);
+    addI(tail_off.size());
+    addI(tail_list.size() + 1);
+    {  // the chase plan (k_chase): offsets per cluster and per CTA, molecule lists
+        size_t ncl = (size_t)std::max(1, nsm / 2);
+        addI(ncl + 1);
+        addI((size_t)nmol + 1);
+        addI(2 * ncl + 1);
+        addI((size_t)nmol + 1);
+    }
     // state
     addD(natT * 3 + natT * 6 + nshT * 2);
     addD((size_t)nnT * 22);
@@ -863,10 +919,60 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.max_iter = o.max_iter;
     b.split = o.precision == 1 ? 1 : 0;
     b.disp = o.dispersion ? 1 : 0;
-    // one-CTA molecules of 34 AOs up to below band_max_nao reduce to tridiagonal form in two
-    // stages, the others (and the whole-grid molecules) in one (AXTB_EIGEN_ONESTAGE=1: all in one stage)
-    b.band_max = o.band_max_nao >= 0 ? o.band_max_nao : DEFAULT_BAND_MAX_NAO;
-    if (std::getenv("AXTB_EIGEN_ONESTAGE")) b.band_max = 0;
+    b.band_max = band_max;
+    b.chase_max = chase_max;
+    vector<int> pair_off, pair_list, solo_off, solo_list;
+    {
+        // the plan: pairs (above CHASE_ROWS AOs) on clusters, then the rest one per CTA, longest
+        // first onto the least loaded; cost ~ time steps (3 n), a pair's steps ~1.3x a CTA's
+        vector<char> is_big(nmol, 0);
+        for (int m : big) is_big[m] = 1;
+        vector<std::pair<double, int>> pairs, solos;
+        for (int m = 0; m < nmol; m++) {
+            int n = m_nao[m];
+            if (is_big[m] || n <= axg::BW + 1 || n >= b.band_max || n > b.chase_max) continue;
+            if (n > axg::CHASE_ROWS) pairs.push_back({3.9 * n, m});
+            else solos.push_back({3.0 * n, m});
+        }
+        nchase = (int)(pairs.size() + solos.size());
+        chase_grid = 2 * std::max(1, nsm / 2);
+        int ncl = chase_grid / 2;
+        auto desc = [](auto& x, auto& y) { return x.first > y.first; };
+        std::sort(pairs.begin(), pairs.end(), desc);
+        std::sort(solos.begin(), solos.end(), desc);
+        using Q = std::priority_queue<std::pair<double, int>, vector<std::pair<double, int>>, std::greater<>>;
+        vector<vector<int>> pl(ncl), sl(chase_grid);
+        vector<double> load(ncl, 0.0);
+        Q qc;
+        for (int c = 0; c < ncl; c++) qc.push({0.0, c});
+        for (auto& x : pairs) {
+            auto top = qc.top();
+            qc.pop();
+            pl[top.second].push_back(x.second);
+            load[top.second] = top.first + x.first;
+            qc.push({load[top.second], top.second});
+        }
+        Q qs;
+        for (int g = 0; g < chase_grid; g++) qs.push({load[g / 2], g});
+        for (auto& x : solos) {
+            auto top = qs.top();
+            qs.pop();
+            sl[top.second].push_back(x.second);
+            qs.push({top.first + x.first, top.second});
+        }
+        pair_off.assign(ncl + 1, 0);
+        for (int c = 0; c < ncl; c++) {
+            pair_off[c + 1] = pair_off[c] + (int)pl[c].size();
+            for (int m : pl[c]) pair_list.push_back(m);
+        }
+        solo_off.assign(chase_grid + 1, 0);
+        for (int g = 0; g < chase_grid; g++) {
+            solo_off[g + 1] = solo_off[g] + (int)sl[g].size();
+            for (int m : sl[g]) solo_list.push_back(m);
+        }
+        pair_list.push_back(0);  // never empty
+        solo_list.push_back(0);
+    }
     // state
     axg::State& s = S;
     s.xyz = ar.take<double>(natT * 3);
@@ -970,6 +1076,14 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     P.nbig = (int)big.size();
     P.small_off = upI(small_off);
     P.small_list = upI(small_list);
+    P.head_off = upI(head_off);
+    P.head_list = upI(head_list);
+    P.tail_off = upI(tail_off);
+    P.tail_list = upI(tail_list);
+    CP.pair_off = upI(pair_off);
+    CP.pair_list = upI(pair_list);
+    CP.solo_off = upI(solo_off);
+    CP.solo_list = upI(solo_list);
     P.m_wk0 = upL(m_wk0);
     P.wk = ar.take<double>(nwk);
     P.m_sq0 = d_sq0;
@@ -1165,9 +1279,9 @@ void AxtbBatch::end_launch() {
 void AxtbBatch::resolve_profile() {
     if (!profiling) return;
     CK(cudaStreamSynchronize(st));
-    unsigned long long cyc[16];
+    unsigned long long cyc[axg::TEAM_CYCLE_SLOTS];
     CK(cudaMemcpyFromSymbol(cyc, axg::g_team_cycles, sizeof cyc));
-    for (int k = 0; k < 16; k++) team_cycles[k] += (double)cyc[k];
+    for (int k = 0; k < axg::TEAM_CYCLE_SLOTS; k++) team_cycles[k] += (double)cyc[k];
     eigen_ms.clear();
     for (auto& r : recs) {
         float ms = 0.f;
@@ -1191,7 +1305,7 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     CK(cudaEventRecord(phase_ev[0], st));
     P.cycles = profiling ? 1 : 0;
     if (profiling) {
-        unsigned long long z[16] = {0};
+        unsigned long long z[TEAM_CYCLE_SLOTS] = {0};
         CK(cudaMemcpyToSymbolAsync(g_team_cycles, z, sizeof z, 0, cudaMemcpyHostToDevice, st));
     }
     const int T = 256;
@@ -1297,9 +1411,19 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
             if (B.solv)
                 LAUNCH("solv_potential", 0, 0, k_solv_potential<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
             LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
-            ph = PH_EIGEN;
-            LAUNCH("team_eigen", eig_flops(act), 0,
-                   CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
+            // the eigen phase: one launch, or three when k_chase takes stage 2 of some molecules
+            LAUNCH("team_eigen", eig_flops(act), 0, {
+                ph = PH_EIGEN;
+                CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st));
+                if (nchase > 0) {
+                    CP.cycles = P.cycles;
+                    k_chase<<<chase_grid, CHASE_THREADS, CHASE_DYN_BYTES, st>>>(B, S, CP);
+                    CK(cudaGetLastError());
+                    ph = PH_EIGEN_TAIL;
+                    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st));
+                    launches += 2;
+                }
+            });
             LAUNCH("mulliken", 0, mat_bytes(act, 12.0),
                    k_mulliken<<<blocks_for((long long)naoT * 32, T), T, 0, st>>>(B, S));
             LAUNCH("moments", 0, 0, k_moments<<<blocks_for(natT, T), T, 0, st>>>(B, S));
@@ -1428,7 +1552,7 @@ __global__ void __launch_bounds__(TEAM_THREADS)
     __syncthreads();
     Team one{0, 1, false};
     mol_overlap(one, B, S, P, 0);
-    mol_eigen(one, B, S, P, 0);
+    mol_eigen(one, B, S, P, 0, false);
     mol_levels(one, B, S, P, 0);  // every orbital energy, not only the ones the filling needs
     if (threadIdx.x == 0 && d_status) *d_status = S.status[0];
 }
@@ -1514,7 +1638,8 @@ extern "C" int axtb_gpu_density_static(const double* d_fock, const double* d_ove
     S.P = d_density;
     B.nmol = 1;
     B.kt = kt;
-    B.band_max = DEFAULT_BAND_MAX_NAO;
+    B.band_max = STATIC_BAND_MAX_NAO;
+    B.chase_max = 0;  // stage 2 in this kernel
     axg::k_density_static<<<1, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES, (cudaStream_t)stream>>>(B, S, P, nao, nalpha, nbeta,
                                                                                               d_status);
     cudaError_t e = cudaGetLastError();

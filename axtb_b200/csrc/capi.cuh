@@ -502,10 +502,14 @@ int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
                                 "back_transform", "c_matrix", "density"};
     // slots 8..13: parts of the tridiagonal reduction (counted instead of slot 1)
     static const char* TP[6] = {"column_update", "householder", "symv", "panel_dots", "combine", "trailing_gemm"};
+    // slots 16..19: the two-stage path's band reduction and bulge chasing (counted instead of
+    // slot 1) and its Q2 and Q1 back-transformations (instead of slot 5)
+    static const char* BP[4] = {"band_reduction", "bulge_chasing", "apply_q2", "apply_q1"};
     double ph[8], tc = 0.0, tt = 0.0;
     for (int k = 0; k < 8; k++) ph[k] = b->team_cycles[k];
     for (int k = 8; k < 14; k++) tt += b->team_cycles[k];
-    ph[1] += tt;
+    ph[1] += tt + b->team_cycles[16] + b->team_cycles[17];
+    ph[5] += b->team_cycles[18] + b->team_cycles[19];
     for (int k = 0; k < 8; k++) tc += ph[k];
     s += "}, \"team_eigen_phases\": {";
     for (int k = 0; k < 8; k++) {
@@ -518,6 +522,12 @@ int axtb_gpu_batch_profile(const AxtbBatch* b, char* buf, size_t len) {
         char tmp[96];
         std::snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", k ? ", " : "", TP[k],
                       tt > 0 ? b->team_cycles[8 + k] / tt : 0.0);
+        s += tmp;
+    }
+    s += "}, \"two_stage_parts\": {";
+    for (int k = 0; k < 4; k++) {
+        char tmp[96];
+        std::snprintf(tmp, sizeof tmp, "%s\"%s\": %.4f", k ? ", " : "", BP[k], tc > 0 ? b->team_cycles[16 + k] / tc : 0.0);
         s += tmp;
     }
     s += "}, \"eigen_launch_ms\": [";

@@ -82,6 +82,7 @@ struct Batch {
     int split;                        // 1: basis-transform and W GEMMs in split precision
     int disp;                         // 0: the D4 term is left out (Options::dispersion = false)
     int band_max;                     // one-CTA molecules below this many AOs reduce to tridiagonal form in two stages
+    int chase_max;                    // ... with stage 2 in its own launch (k_chase) up to this many AOs (0: none)
 };
 
 // per-geometry and per-iteration device state

@@ -382,57 +382,108 @@ __device__ void team_sb2st(const Team& t, const double* A, long long lda, int n,
 }
 
 // ---------------------------------------------------------------------------------- back
-// Z <- Q2 Z (Z: n x k, leading dimension ldz) from the stage-2 reflectors
+// Z <- Q2 Z (Z: n x k, leading dimension ldz) from the stage-2 reflectors, one CTA. Per group of
+// 32 sweeps (from the last) and step s (ascending; this order respects every overlap), the 32
+// reflectors of the group at step s form an explicit 64 x 64 orthogonal block X_s on the rows
+// from J + 1 + s BW: built in shared memory (thread = column, the reflectors in order), then
+// applied in place, Z[w0 : w0 + 64] <- X_s Z[w0 : w0 + 64], on the FP64 tensor cores with X_s
+// kept in shared memory and Z streamed through a three-deep ring of 64 x 16 column chunks
+// (cp.async; each chunk is read, multiplied and stored before the ring reuses its slot).
+constexpr int Q2_XLD = 68;  // X_s row stride (doubles): conflict-free fragment loads
+constexpr int Q2_ZC = 16;   // Z columns per chunk
+constexpr int Q2_ZLD = 20;  // chunk row stride (doubles)
+constexpr int Q2_STAGES = 3;
+static_assert(64 * Q2_XLD + Q2_STAGES * 64 * Q2_ZLD <= SMEM_WORK && BW * BW <= Q2_STAGES * 64 * Q2_ZLD,
+              "X_s and the chunk ring (or the staged reflectors) fit the work area");
+
+__device__ void cta_q2_block(const double* X, double* Z, long long ldz, int rows, int k) {
+    double* ring = s_work + 64 * Q2_XLD;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = warp & 3, wn = warp >> 2;  // warp tile: rows wm*16 .. +16, chunk columns wn*8 .. +8
+    const int lr = lane >> 2, lc = lane & 3;
+    const int nch = (k + Q2_ZC - 1) / Q2_ZC;
+    auto issue = [&](int ch) {
+        if (ch < nch) {
+            double* st = ring + (ch % Q2_STAGES) * 64 * Q2_ZLD;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                int e = threadIdx.x + q * 256;
+                int r = e & 63, c = e >> 6;
+                int gc = ch * Q2_ZC + c;
+                bool ok = r < rows && gc < k;
+                cp_async8(st + r * Q2_ZLD + c, ok ? Z + r + (long long)gc * ldz : Z, ok);
+            }
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    issue(1);
+    for (int ch = 0; ch < nch; ch++) {
+        cp_async_wait<1>();  // this thread's copies of chunk ch have landed
+        __syncthreads();     // everyone's have; the slot of chunk ch - 1 is free
+        issue(ch + 2);
+        const double* zs = ring + (ch % Q2_STAGES) * 64 * Q2_ZLD;
+        double acc[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+        for (int kk = 0; kk < 64; kk += 4) {
+            double bf = zs[(kk + lc) * Q2_ZLD + wn * 8 + lr];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                double af = X[(wm * 16 + i * 8 + lr) * Q2_XLD + kk + lc];
+                dmma_8x8x4(acc[i][0], acc[i][1], af, bf);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            int r = wm * 16 + i * 8 + lr;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int gc = ch * Q2_ZC + wn * 8 + lc * 2 + h;
+                if (r < rows && gc < k) Z[r + (long long)gc * ldz] = acc[i][h];
+            }
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();  // the work area is free for the next block
+}
+
 __device__ void team_apply_q2(const Team& t, int n, int k, double* Z, long long ldz, const double* refl, double* wk) {
     if (n <= 2 || k <= 0) return;
-    double* blocks = wk + band_off_blocks(n);
-    double* tmp = wk + band_off_tmp(n);
     const int nsweep = n - 2;
+    double* X = s_work;  // 64 x Q2_XLD
     for (int J = ((nsweep - 1) / BW) * BW; J >= 0; J -= BW) {
         int ns = band_steps(n - J);  // steps of the group's first sweep (the longest)
-        // explicit block of step s: X = H_{J,s} H_{J+1,s} .. H_{J+31,s} on the 64 rows from
-        // J + 1 + s BW, two blocks at a time in shared memory (thread = column)
-        auto Xs = reinterpret_cast<double(*)[64][65]>(s_work);
-        for (int s0 = 0; s0 < ns; s0 += 2) {
-            int h = threadIdx.x >> 7, col = threadIdx.x & 127;
-            int s = s0 + h;
-            if (col < 64 && s < ns) {
-                double(*X)[65] = Xs[h];
-                for (int r = 0; r < 64; r++) X[r][col] = r == col ? 1.0 : 0.0;
-                int w0 = J + 1 + s * BW;
-                for (int dl = BW - 1; dl >= 0; dl--) {
-                    int j = J + dl;
-                    if (j >= nsweep || s >= band_steps(n - j)) continue;
-                    const double* rf = refl + band_refl_index(n, j, s) * BW;
-                    double tc = rf[0];
-                    if (tc == 0.0) continue;
-                    int lo = j + 1 + s * BW, L = min(BW, n - lo);
-                    int r0 = lo - w0;  // = dl
-                    double w = X[r0][col];
-                    for (int r = 1; r < L; r++) w = fma(rf[r], X[r0 + r][col], w);
-                    double tw = tc * w;
-                    X[r0][col] -= tw;
-                    for (int r = 1; r < L; r++) X[r0 + r][col] -= tw * rf[r];
-                }
-            }
-            __syncthreads();
-            if (col < 64 && s < ns) {
-                double* dst = blocks + (long long)s * 64 * 64;
-                for (int r = 0; r < 64; r++) dst[r + col * 64] = Xs[h][r][col];
-            }
-            __syncthreads();
-        }
-        // apply the group's blocks in ascending steps: Z[w0 : w0 + 64] <- X_s Z[w0 : w0 + 64]
         for (int s = 0; s < ns; s++) {
             int w0 = J + 1 + s * BW, rows = min(64, n - w0);
             if (rows <= 0) break;
-            team_gemm(t, false, false, rows, k, rows, 1.0, blocks + (long long)s * 64 * 64, 64, Z + w0, ldz, 0.0, tmp,
-                      64);
-            for (long long q = threadIdx.x; q < (long long)rows * k; q += blockDim.x) {
-                int r = (int)(q % rows), c = (int)(q / rows);
-                Z[w0 + r + (long long)c * ldz] = tmp[r + (long long)c * 64];
+            // the group's reflectors at step s, staged in shared memory by every thread (the
+            // chunk ring's space, free until the product), tau = 0 for sweeps without the step
+            double* R = s_work + 64 * Q2_XLD;
+            for (int q = threadIdx.x; q < BW * BW; q += blockDim.x) {
+                int j = J + q / BW;
+                bool has = j < nsweep && s < band_steps(n - j);
+                R[q] = has ? refl[band_refl_index(n, j, s) * BW + q % BW] : 0.0;
             }
             __syncthreads();
+            // X_s = H_{J,s} H_{J+1,s} .. H_{J+31,s} on the 64 rows from w0 (thread = column)
+            int col = threadIdx.x;
+            if (col < 64) {
+                for (int r = 0; r < 64; r++) X[r * Q2_XLD + col] = r == col ? 1.0 : 0.0;
+                for (int dl = BW - 1; dl >= 0; dl--) {
+                    const double* rf = R + dl * BW;
+                    double tc = rf[0];
+                    if (tc == 0.0) continue;
+                    int lo = J + dl + 1 + s * BW, L = min(BW, n - lo);
+                    int r0 = lo - w0;  // = dl
+                    double w = X[r0 * Q2_XLD + col];
+                    for (int r = 1; r < L; r++) w = fma(rf[r], X[(r0 + r) * Q2_XLD + col], w);
+                    double tw = tc * w;
+                    X[r0 * Q2_XLD + col] -= tw;
+                    for (int r = 1; r < L; r++) X[(r0 + r) * Q2_XLD + col] -= tw * rf[r];
+                }
+            }
+            __syncthreads();
+            cta_q2_block(X, Z + w0, ldz, rows, k);
         }
     }
 }

@@ -5,7 +5,9 @@
 //   PH_EEQ      EEQ start charges from the Cholesky factor of the EEQ matrix
 //               (crates/axtb/src/eeq.rs:43-77, bordered system solved by its Schur complement)
 //   PH_EIGEN    F' = L^-1 F L^-T, eigenvalues, tblite Fermi filling, occupied eigenvectors,
-//               C = L^-T Q Z and P = C f C^T (crates/axtb/src/xtb.rs:997-1038)
+//               C = L^-T Q Z and P = C f C^T (crates/axtb/src/xtb.rs:997-1038); for a molecule
+//               whose band is chased on chip (k_chase) only F' and stage 1 of the reduction
+//   PH_EIGEN_TAIL  the rest of those molecules' eigen phase, after k_chase
 //   PH_WDENS    W = C (f e) C^T (crates/axtb/src/xtb.rs:688-696)
 //   PH_LEVELS   the orbital energies above the ones the SCF needed, from the last tridiagonal
 //               matrix (all levels, as the reference's eigensolver returns them for the result)
@@ -16,13 +18,17 @@
 
 namespace axg {
 
-enum { PH_OVERLAP = 0, PH_EEQ = 1, PH_EIGEN = 2, PH_WDENS = 3, PH_LEVELS = 4 };
+enum { PH_OVERLAP = 0, PH_EEQ = 1, PH_EIGEN = 2, PH_WDENS = 3, PH_LEVELS = 4, PH_EIGEN_TAIL = 5 };
 
 struct TeamPlan {
     const int* big;        // molecules run by the whole grid
     int nbig;
     const int* small_off;  // per CTA: range into small_list
     const int* small_list;
+    const int* head_off;   // the same for PH_EIGEN (balanced on its own cost model) ...
+    const int* head_list;
+    const int* tail_off;   // ... and for PH_EIGEN_TAIL
+    const int* tail_list;
     const long long* m_wk0;   // per-molecule workspace offsets into wk
     double* wk;
     const long long* m_sq0;   // per-molecule nat^2 offsets (EEQ planes)
@@ -137,7 +143,19 @@ __device__ void mol_fermi(const Team& t, const Batch& B, State& S, int m, const 
     t.sync();
 }
 
-__device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
+// the two-stage reduction needs a band stage: a matrix of at most BW + 1 rows already is a band,
+// and the one-stage path keeps the bits that small chaotic SCFs follow
+__device__ __forceinline__ bool two_stage(const Team& t, const Batch& B, int n) {
+    return !t.global && n > BW + 1 && n < B.band_max;
+}
+// stage 2 of the two-stage reduction in its own launch with the band in shared memory (k_chase)
+__device__ __forceinline__ bool chased_on_chip(const Team& t, const Batch& B, int n) {
+    return two_stage(t, B, n) && n <= B.chase_max;
+}
+
+// after_chase: the part after k_chase of a molecule whose bulge chasing ran on chip (from its
+// tridiagonal matrix on); otherwise the whole eigen phase, or for such a molecule the part before
+__device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m, bool after_chase) {
     int n = B.m_nao[m], ao0 = B.m_ao0[m];
     long long mat = B.m_mat0[m];
     double* wk = P.wk + P.m_wk0[m];
@@ -145,6 +163,12 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* X = S.scr1 + mat;
     double* Fp = S.Fp + mat;
     long long t0__ = clock64(), tstart = t0__;
+    double* d = S.dtri + ao0;
+    double* e = S.etri + ao0;
+    double* tau = S.tau + ao0;
+    const int nsl = symv_slots(n);
+    const bool band = two_stage(t, B, n);
+    if (!after_chase) {
     // F' = L^-1 F L^-T (L^-1 is lower triangular; F' is symmetric and only its lower triangle is
     // used: the tiles on and below the diagonal are computed)
     // split precision for the basis transform only: an error there perturbs F', whose exactly
@@ -156,23 +180,20 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     team_gemm(t, false, true, n, n, n, 1.0, X, n, Linv, n, 0.0, Fp, n, GEMM_B_UPPER | GEMM_LOWER_TILES | sp);
     t.sync();
     TEAM_PHASE(0);
-    double* d = S.dtri + ao0;
-    double* e = S.etri + ao0;
-    double* tau = S.tau + ao0;
     double* vbuf = wk;
     double* pbuf = wk + n;
     double* ppart = wk + 2 * n;
-    const int nsl = symv_slots(n);
-    // the two-stage path needs a band stage: a matrix of at most BW + 1 rows already is a band,
-    // and the one-stage path keeps the bits that small chaotic SCFs follow
-    const bool band = !t.global && n > BW + 1 && n < B.band_max;
     if (band) {
         // one CTA: two-stage reduction (dense -> band on GEMMs, band -> tridiagonal by bulge
         // chasing), the stage-2 reflectors in the W plane (free until the gradient's W)
         team_sy2sb(t, Fp, n, n, tau, wk);
-        TEAM_PHASE(8);
+        TEAM_PHASE(16);
+        if (n <= B.chase_max) {  // stage 2 and the rest in the next two launches
+            if (P.cycles && t.tid() == 0) S.mol_cyc[m] = (double)(clock64() - tstart);
+            return;
+        }
         team_sb2st(t, Fp, n, n, d, e, wk, S.W + mat);
-        TEAM_PHASE(10);
+        TEAM_PHASE(17);
     } else {
         double* Vp = wk + 2 * n + (long long)nsl * n;  // the back-transform's vb area (64 n)
         team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
@@ -180,6 +201,7 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
         if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     }
     TEAM_PHASE(1);
+    }
     double* emo = S.emo + ao0;
     // eigenvalues: the lowest ceil(n_occ) + a margin first; the levels above get the Gershgorin
     // bound (occupation exactly 0 at any sensible kT). If the highest computed level still holds
@@ -212,7 +234,9 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     double* y2 = y + 64LL * n;
     if (band) {
         team_apply_q2(t, n, k, Zm, n, S.W + mat, wk);
+        TEAM_PHASE(18);
         team_apply_q1(t, Fp, n, n, k, Zm, n, wk);
+        TEAM_PHASE(19);
     } else {
         team_backtransform(t, Fp, n, tau, n, k, Zm, n, vb, tb, gm, y, y2);
     }
@@ -230,7 +254,11 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
     team_mirror_lower(t, S.P + mat, n, 0, n);
     t.sync();
     TEAM_PHASE(7);
-    if (P.cycles && t.tid() == 0) S.mol_cyc[m] = (double)(clock64() - tstart);
+    if (P.cycles && t.tid() == 0) {
+        double c = (double)(clock64() - tstart);
+        if (after_chase) S.mol_cyc[m] += c;  // after the part before and the chase
+        else S.mol_cyc[m] = c;
+    }
 }
 
 __device__ void mol_wdens(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m) {
@@ -264,7 +292,7 @@ __device__ void mol_levels(const Team& t, const Batch& B, State& S, const TeamPl
 }
 
 __device__ __forceinline__ bool phase_wants(const State& S, int phase, int m) {
-    if (phase == PH_EIGEN) return S.active[m] != 0;
+    if (phase == PH_EIGEN || phase == PH_EIGEN_TAIL) return S.active[m] != 0;
     if (phase == PH_WDENS) return S.conv[m] != 0;
     return true;
 }
@@ -273,7 +301,10 @@ __device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan&
     switch (phase) {
         case PH_OVERLAP: mol_overlap(t, B, S, P, m); break;
         case PH_EEQ: mol_eeq(t, B, S, P, m); break;
-        case PH_EIGEN: mol_eigen(t, B, S, P, m); break;
+        case PH_EIGEN:
+        case PH_EIGEN_TAIL:
+            if (phase == PH_EIGEN || chased_on_chip(t, B, B.m_nao[m])) mol_eigen(t, B, S, P, m, phase == PH_EIGEN_TAIL);
+            break;
         case PH_WDENS: mol_wdens(t, B, S, P, m); break;
         case PH_LEVELS: mol_levels(t, B, S, P, m); break;
     }
@@ -288,8 +319,10 @@ __global__ void __launch_bounds__(TEAM_THREADS, 2) k_team(Batch B, State S, Team
         if (phase_wants(S, phase, m)) run_mol(g, B, S, P, phase, m);  // uniform across the grid
     }
     Team one{0, 1, false};
-    for (int i = P.small_off[blockIdx.x]; i < P.small_off[blockIdx.x + 1]; i++) {
-        int m = P.small_list[i];
+    const int* off = phase == PH_EIGEN ? P.head_off : phase == PH_EIGEN_TAIL ? P.tail_off : P.small_off;
+    const int* list = phase == PH_EIGEN ? P.head_list : phase == PH_EIGEN_TAIL ? P.tail_list : P.small_list;
+    for (int i = off[blockIdx.x]; i < off[blockIdx.x + 1]; i++) {
+        int m = list[i];
         if (phase_wants(S, phase, m)) run_mol(one, B, S, P, phase, m);
     }
 }

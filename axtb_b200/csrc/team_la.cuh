@@ -25,7 +25,8 @@ constexpr int TEAM_THREADS = 256;
 
 // SM-cycle counters of the eigen phase's parts (instrumentation, read by the profiler):
 // 0..7 the phases of the eigen step, 8..13 the parts of the tridiagonal reduction
-__device__ unsigned long long g_team_cycles[16];
+constexpr int TEAM_CYCLE_SLOTS = 24;
+__device__ unsigned long long g_team_cycles[TEAM_CYCLE_SLOTS];
 
 struct Team {
     int rank;     // CTA rank in the team

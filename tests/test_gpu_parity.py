@@ -192,3 +192,24 @@ def test_autotuned_schedule_gives_the_same_results(engine, tmp_path, monkeypatch
             assert a.status == b.status == 0
             assert abs(a.energy - b.energy) < E_TOL
             assert np.abs(a.gradient - b.gradient).max() < G_TOL
+
+
+def test_stage2_on_chip_gives_the_same_bits(engine, monkeypatch):
+    """Stage 2 of the two-stage reduction in shared memory (k_chase: one CTA, or a cluster pair
+    above 440 AOs) does the global-memory chase's arithmetic in the same order: identical energies,
+    gradients and iteration counts."""
+    from axtb_b200 import structures as S
+
+    mols = [S.water_cluster(90, seed=3), S.water_cluster(60, seed=4), S.alkane(40, seed=5), S.water_cluster(12, seed=6),
+            S.alkane(6, seed=7), S.water_cluster(75, seed=8)]
+    nao = [engine.basis_size(z)[1] for z, _ in mols]
+    assert max(nao) > 440 and min(nao) <= 64  # a cluster pair and one-CTA bands
+    sched = {"band_max_nao": 1 << 30}
+    chip = engine.Batch(mols, accuracy=1e-4, **sched).run(gradient=True)
+    monkeypatch.setenv("AXTB_STAGE2_IN_TEAM", "1")
+    team = engine.Batch(mols, accuracy=1e-4, **sched).run(gradient=True)
+    for a, b in zip(chip, team):
+        assert a.status == b.status == 0
+        assert a.iterations == b.iterations
+        assert a.energy == b.energy
+        assert np.array_equal(a.gradient, b.gradient)
