@@ -92,15 +92,14 @@ def basis_size(numbers):
 
 
 class _ResultBuffers:
-    def __init__(self, nat, nsh, nao=0):
-        self.grad = np.zeros((nat, 3))
-        self.q = np.zeros(nat)
-        self.dip = np.zeros(3)
-        self.qsh = np.zeros(nsh)
-        self.dp = np.zeros((nat, 3))
-        self.qp = np.zeros((nat, 6))
+    def __init__(self, nat, nsh, nao=0, views=None):
+        """One molecule's output arrays: its own, or `views` (grad, q, dip, qsh, dp, qp, emo, focc,
+        focca) into a batch's field-wise arrays."""
+        if views is None:
+            views = (np.zeros((nat, 3)), np.zeros(nat), np.zeros(3), np.zeros(nsh), np.zeros((nat, 3)),
+                     np.zeros((nat, 6)), np.zeros(nao), np.zeros(nao), np.zeros(nao))
+        self.grad, self.q, self.dip, self.qsh, self.dp, self.qp, self.emo, self.focc, self.focca = views
         self.nao = nao
-        self.emo, self.focc, self.focca = np.zeros(nao), np.zeros(nao), np.zeros(nao)
         self.res = _lib.AxtbResult()
         self.bind(False)
 
@@ -118,27 +117,30 @@ class _ResultBuffers:
         return r
 
     def result(self, gradient: bool) -> SinglePoint:
-        r = self.res
-        used = MIXER_USED[r.mixer_used]
-        if used == "diis-fallback":
-            attempts = [("broyden", r.fallback_iterations, False), ("diis", r.iterations if r.converged else
-                                                                    r.iterations - r.fallback_iterations,
-                                                                    bool(r.converged))]
-        else:
-            attempts = [(used, r.iterations, bool(r.converged))]
-        return SinglePoint(energy=r.energy, gradient=self.grad.copy() if gradient else None, charges=self.q.copy(),
-                           dipole=self.dip.copy(), qsh=self.qsh.copy(), dpat=self.dp.copy(), qpat=self.qp.copy(),
-                           terms=dict(zip(TERM_NAMES, list(r.terms)), solvation=r.solvation),
-                           iterations=r.iterations,
-                           converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
-                           residual=r.residual, mixer_used=used,
-                           emo=self.emo.copy() if self.levels else None,
-                           focc=self.focc.copy() if self.levels else None,
-                           focc_alpha=self.focca.copy() if self.levels else None,
-                           fermi_levels=(r.fermi_levels[0], r.fermi_levels[1]),
-                           electronic_temperature=r.electronic_temperature,
-                           start="previous" if r.warm_start else "guess", attempts=attempts,
-                           timings=dict(zip(("setup", "scf", "gradient", "total"), list(r.timings))))
+        return _single_point(self.res, self.grad.copy() if gradient else None, self.q.copy(), self.dip.copy(),
+                             self.qsh.copy(), self.dp.copy(), self.qp.copy(),
+                             *((self.emo.copy(), self.focc.copy(), self.focca.copy()) if self.levels else (None,) * 3))
+
+
+def _single_point(r, grad, q, dip, qsh, dp, qp, emo, focc, focca) -> SinglePoint:
+    """A SinglePoint from the ABI result `r` and arrays the caller owns."""
+    used = MIXER_USED[r.mixer_used]
+    if used == "diis-fallback":
+        attempts = [("broyden", r.fallback_iterations, False), ("diis", r.iterations if r.converged else
+                                                                r.iterations - r.fallback_iterations,
+                                                                bool(r.converged))]
+    else:
+        attempts = [(used, r.iterations, bool(r.converged))]
+    return SinglePoint(energy=r.energy, gradient=grad, charges=q, dipole=dip, qsh=qsh, dpat=dp, qpat=qp,
+                       terms=dict(zip(TERM_NAMES, list(r.terms)), solvation=r.solvation),
+                       iterations=r.iterations,
+                       converged=bool(r.converged), status=r.status, energy_change=r.energy_change,
+                       residual=r.residual, mixer_used=used,
+                       emo=emo, focc=focc, focc_alpha=focca,
+                       fermi_levels=(r.fermi_levels[0], r.fermi_levels[1]),
+                       electronic_temperature=r.electronic_temperature,
+                       start="previous" if r.warm_start else "guess", attempts=attempts,
+                       timings=dict(zip(("setup", "scf", "gradient", "total"), list(r.timings))))
 
 
 # SCC mixers by name (crates/axtb/src/scf/mixing.rs:202-214: case-insensitive, "pulay" = DIIS;
@@ -288,16 +290,34 @@ class Batch:
         self._b = b
         self.nmol = len(molecules)
         self.natoms = np.array([len(z) for z, _ in self.mols])
-        self._bufs = [_ResultBuffers(len(z), *basis_size(z)) for z, _ in self.mols]
+        # the outputs field by field over the whole batch (one copy per field after a run), each
+        # molecule's ABI result pointing at its rows
+        sizes = np.array([basis_size(z) for z, _ in self.mols], dtype=np.int64).reshape(-1, 2)
+        self._at = np.concatenate([[0], np.cumsum(self.natoms)])
+        self._sh = np.concatenate([[0], np.cumsum(sizes[:, 0])])
+        self._ao = np.concatenate([[0], np.cumsum(sizes[:, 1])])
+        natT, nshT, naoT = int(self._at[-1]), int(self._sh[-1]), int(self._ao[-1])
+        self._all = (np.zeros((natT, 3)), np.zeros(natT), np.zeros((self.nmol, 3)), np.zeros(nshT),
+                     np.zeros((natT, 3)), np.zeros((natT, 6)), np.zeros(naoT), np.zeros(naoT), np.zeros(naoT))
+        self._bufs = []
+        for i in range(self.nmol):
+            a, sh, ao = slice(self._at[i], self._at[i + 1]), slice(self._sh[i], self._sh[i + 1]), slice(self._ao[i], self._ao[i + 1])
+            g, q, d, qs, dp, qp, emo, focc, focca = self._all
+            views = (g[a], q[a], d[i], qs[sh], dp[a], qp[a], emo[ao], focc[ao], focca[ao])
+            self._bufs.append(_ResultBuffers(int(self.natoms[i]), int(sizes[i, 0]), int(sizes[i, 1]), views))
         self._res = (_lib.AxtbResult * self.nmol)()
+        self._bound = None  # the levels flag the results were last bound with
 
     def run(self, positions=None, gradient=True, levels=False):
         """Single points of every molecule (positions: list of (nat, 3) arrays or None for the
         set-up geometries); returns a list of SinglePoint (status per molecule). `levels`: also
         every orbital energy and the occupations of each molecule."""
         lib = _lib.load()
-        for i, bf in enumerate(self._bufs):
-            self._res[i] = bf.bind(levels)
+        levels = bool(levels)
+        if self._bound != levels:  # the pointers stay valid between runs
+            for i, bf in enumerate(self._bufs):
+                self._res[i] = bf.bind(levels)
+            self._bound = levels
         st = np.zeros(self.nmol, dtype=np.int32)
         xp = None
         if positions is not None:
@@ -306,10 +326,20 @@ class Batch:
         rc = lib.axtb_gpu_batch_run(self._b, xp, int(bool(gradient)), self._res, st.ctypes.data_as(C.POINTER(C.c_int32)))
         if rc != 0:
             raise AxtbError(rc, _lib.last_error(None))
+        # one copy per field (the gradients and the levels only when asked for), then each
+        # molecule's rows as views of the copies
+        g, q, d, qs, dp, qp, emo, focc, focca = self._all
+        g = g.copy() if gradient else None
+        q, d, qs, dp, qp = q.copy(), d.copy(), qs.copy(), dp.copy(), qp.copy()
+        if levels:
+            emo, focc, focca = emo.copy(), focc.copy(), focca.copy()
         out = []
-        for i, bf in enumerate(self._bufs):
-            bf.res = self._res[i]
-            out.append(bf.result(gradient))
+        at, sh, ao = self._at, self._sh, self._ao
+        for i in range(self.nmol):
+            a0, a1, s0, s1 = at[i], at[i + 1], sh[i], sh[i + 1]
+            lv = (emo[ao[i]:ao[i + 1]], focc[ao[i]:ao[i + 1]], focca[ao[i]:ao[i + 1]]) if levels else (None,) * 3
+            out.append(_single_point(self._res[i], g[a0:a1] if gradient else None, q[a0:a1], d[i], qs[s0:s1],
+                                     dp[a0:a1], qp[a0:a1], *lv))
         return out
 
     def run_device(self, d_positions: int, d_energy: int, d_gradient: int, gradient=True):

@@ -5,11 +5,14 @@
 // nuclear gradient. Follows crates/axtb/src/integrals.rs:28-367 (S, D, Q), 400-521 (ket
 // derivatives), 991-1006 (shift to the bra) and crates/axtb/src/hamiltonian.rs:77-94 (H0),
 // 101-223 (gradient). One thread per atom pair; blocks are written straight into the AO
-// matrices (each element has exactly one writer), gradient pieces into a per-pair buffer. Each
-// shell pair runs in a function templated on its two angular momenta (a switch per pair), so the
-// Cartesian accumulators have compile-time sizes and stay in registers for s and p shells (at
-// most 168 registers a thread: three CTAs of 128 per SM); d-shell pairs, in their own
-// non-inlined functions, spill what does not fit.
+// matrices (each element has exactly one writer), gradient pieces into a per-pair buffer. In the
+// gradient each shell pair runs in a function templated on its two angular momenta (a switch per
+// pair), so the Cartesian accumulators have compile-time sizes and stay in registers for s and p
+// shells (at most 168 registers a thread: three CTAs of 128 per SM); d-shell pairs, in their own
+// non-inlined functions, spill what does not fit. The S, D, Q kernel keeps the generic loops: the
+// same templating there gave the integrals other last bits (the compiler fuses the recursion's
+// products differently once the angular momenta are constants), and those bits steer a few
+// chaotic SCFs that axtb's records pin.
 #pragma once
 #include "common.cuh"
 #include "k_geometry.cuh"
@@ -88,6 +91,24 @@ __device__ __forceinline__ void os_1d(double rpa, double rpb, double h, double (
     }
 }
 
+// the same table for runtime la, lb (the S, D, Q integrals: their bits steer a few chaotic SCFs,
+// so they keep this form)
+__device__ __forceinline__ void os_1d(int la, int lb, double rpa, double rpb, double h, double t[6][6]) {
+    t[0][0] = 1.0;
+    if (la >= 1) {
+        t[1][0] = rpa;
+        for (int i = 1; i < la; i++) t[i + 1][0] = rpa * t[i][0] + i * h * t[i - 1][0];
+    }
+    if (lb >= 1) {
+        t[0][1] = rpb;
+        for (int i = 1; i <= la; i++) t[i][1] = rpb * t[i][0] + i * h * t[i - 1][0];
+        for (int j = 1; j < lb; j++) {
+            t[0][j + 1] = rpb * t[0][j] + j * h * t[0][j - 1];
+            for (int i = 1; i <= la; i++) t[i][j + 1] = rpb * t[i][j] + h * (i * t[i - 1][j] + j * t[i][j - 1]);
+        }
+    }
+}
+
 __device__ __forceinline__ void traceless6(double* q) {
     double tr = 0.5 * (q[0] + q[2] + q[5]);
     q[0] = 1.5 * q[0] - tr;
@@ -113,57 +134,32 @@ __device__ __forceinline__ bool pair_screened(double a, double b, double r2, dou
     return a * b * r2 / (a + b) > intcut * (1.0 + 1e-10);
 }
 
-__device__ __forceinline__ void shift_bra(const double vec[3], double s, const double* di, const double* qi, double* dj,
-                                          double* qj) {
-    for (int k = 0; k < 3; k++) dj[k] = di[k] + vec[k] * s;
-    qj[0] = 2.0 * vec[0] * di[0] + vec[0] * vec[0] * s;
-    qj[1] = vec[0] * di[1] + vec[1] * di[0] + vec[0] * vec[1] * s;
-    qj[2] = 2.0 * vec[1] * di[1] + vec[1] * vec[1] * s;
-    qj[3] = vec[0] * di[2] + vec[2] * di[0] + vec[0] * vec[2] * s;
-    qj[4] = vec[1] * di[2] + vec[2] * di[1] + vec[1] * vec[2] * s;
-    qj[5] = 2.0 * vec[2] * di[2] + vec[2] * vec[2] * s;
-    traceless6(qj);
-    for (int k = 0; k < 6; k++) qj[k] += qi[k];
-}
-
-// S, D (about R_i) and traceless Q (about R_i) of (bra cj at R_j, ket ci at R_i), vec = R_i - R_j,
-// for shells of angular momenta LJ, LI (compile-time sizes: the Cartesian accumulators stay in
-// registers for s and p shells), written with H0 = S hij into the AO matrices at element e1 =
-// (mu, nu) and, off the diagonal atom pair, the transposed element with D and Q shifted to R_j
-template <int LI, int LJ>
-__device__ __noinline__ void shell_pair_integrals(const Batch& B, State& S, const Shl& cj, const Shl& ci, const double vec[3],
-                                     double hij, bool onsite, int mu0, int nu0, int n, long long mat) {
-    constexpr int NCI = (LI + 1) * (LI + 2) / 2, NCJ = (LJ + 1) * (LJ + 2) / 2;
-    constexpr int NSI = 2 * LI + 1, NSJ = 2 * LJ + 1;
-    const long long nn = B.nnT;
+// S, D (about R_i) and traceless Q (about R_i) of (bra cj at R_j, ket ci at R_i), vec = R_i - R_j.
+// Outputs in spherical order, block index jm + nsph(lj)*im.
+__device__ void multipole_block(const Shl& cj, const Shl& ci, const double vec[3], double intcut, double* s, double* d,
+                                double* q) {
     double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
-    double cart[NCJ * NCI][10];
-#pragma unroll
-    for (int p = 0; p < NCJ * NCI; p++)
-#pragma unroll
+    int li = ci.l, lj = cj.l, ncj = ncart(lj), nci = ncart(li);
+    double cart[36][10];
+    for (int p = 0; p < ncj * nci; p++)
         for (int x = 0; x < 10; x++) cart[p][x] = 0.0;
-    double t[3][LI + 3][LJ + 1];
+    double t[3][6][6];
     for (int ip = 0; ip < ci.np; ip++)
         for (int jp = 0; jp < cj.np; jp++) {
             double ai = ci.a[ip], aj = cj.a[jp], oab, pre;
-            if (!prim_pref(ai, aj, r2, B.intcut, oab, pre)) continue;
-#pragma unroll
-            for (int k = 0; k < 3; k++) os_1d<LI + 2, LJ>(-vec[k] * aj * oab, vec[k] * ai * oab, 0.5 * oab, t[k]);
+            if (!prim_pref(ai, aj, r2, intcut, oab, pre)) continue;
+            for (int k = 0; k < 3; k++) os_1d(li + 2, lj, -vec[k] * aj * oab, vec[k] * ai * oab, 0.5 * oab, t[k]);
             double cc = ci.c[ip] * cj.c[jp] * pre;
-#pragma unroll
-            for (int ic = 0; ic < NCI; ic++) {
+            for (int ic = 0; ic < nci; ic++) {
                 int ea[3];
-                cart_exp(LI, ic, ea);
-#pragma unroll
-                for (int jc = 0; jc < NCJ; jc++) {
+                cart_exp(li, ic, ea);
+                for (int jc = 0; jc < ncj; jc++) {
                     int eb[3];
-                    cart_exp(LJ, jc, eb);
+                    cart_exp(lj, jc, eb);
                     double v[3][3];
-#pragma unroll
                     for (int k = 0; k < 3; k++)
-#pragma unroll
                         for (int mm = 0; mm < 3; mm++) v[k][mm] = t[k][ea[k] + mm][eb[k]];
-                    double* c = cart[jc + NCJ * ic];
+                    double* c = cart[jc + ncj * ic];
                     c[0] += cc * v[0][0] * v[1][0] * v[2][0];
                     c[1] += cc * v[0][1] * v[1][0] * v[2][0];
                     c[2] += cc * v[0][0] * v[1][1] * v[2][0];
@@ -177,49 +173,40 @@ __device__ __noinline__ void shell_pair_integrals(const Batch& B, State& S, cons
                 }
             }
         }
-#pragma unroll
-    for (int im = 0; im < NSI; im++)
-#pragma unroll
-        for (int jm = 0; jm < NSJ; jm++) {
+    int nsj = nsph(lj), nsi = nsph(li);
+    for (int im = 0; im < nsi; im++)
+        for (int jm = 0; jm < nsj; jm++) {
             double o[10];
-#pragma unroll
             for (int x = 0; x < 10; x++) o[x] = 0.0;
-#pragma unroll
-            for (int ic = 0; ic < NCI; ic++) {
-                double ti = sph_t(LI, im, ic);
+            for (int ic = 0; ic < nci; ic++) {
+                double ti = sph_t(li, im, ic);
                 if (ti == 0.0) continue;
-#pragma unroll
-                for (int jc = 0; jc < NCJ; jc++) {
-                    double tj = sph_t(LJ, jm, jc);
+                for (int jc = 0; jc < ncj; jc++) {
+                    double tj = sph_t(lj, jm, jc);
                     if (tj == 0.0) continue;
-#pragma unroll
-                    for (int x = 0; x < 10; x++) o[x] += tj * ti * cart[jc + NCJ * ic][x];
+                    for (int x = 0; x < 10; x++) o[x] += tj * ti * cart[jc + ncj * ic][x];
                 }
             }
-            double sv = o[0];
-            double dv[3] = {o[1], o[2], o[3]};
+            int k = jm + nsj * im;
+            s[k] = o[0];
+            for (int x = 0; x < 3; x++) d[3 * k + x] = o[1 + x];
             double qq[6] = {o[4], o[5], o[6], o[7], o[8], o[9]};
             traceless6(qq);
-            int mu = mu0 + jm, nu = nu0 + im;
-            long long e1 = mat + mu + (long long)nu * n;
-            S.S[e1] = sv;
-            S.H0[e1] = sv * hij;
-#pragma unroll
-            for (int x = 0; x < 3; x++) S.D[x * nn + e1] = dv[x];
-#pragma unroll
-            for (int x = 0; x < 6; x++) S.Q[x * nn + e1] = qq[x];
-            if (!onsite) {
-                double dj[3], qj[6];
-                shift_bra(vec, sv, dv, qq, dj, qj);
-                long long e2 = mat + nu + (long long)mu * n;
-                S.S[e2] = sv;
-                S.H0[e2] = sv * hij;
-#pragma unroll
-                for (int x = 0; x < 3; x++) S.D[x * nn + e2] = dj[x];
-#pragma unroll
-                for (int x = 0; x < 6; x++) S.Q[x * nn + e2] = qj[x];
-            }
+            for (int x = 0; x < 6; x++) q[6 * k + x] = qq[x];
         }
+}
+
+__device__ __forceinline__ void shift_bra(const double vec[3], double s, const double* di, const double* qi, double* dj,
+                                          double* qj) {
+    for (int k = 0; k < 3; k++) dj[k] = di[k] + vec[k] * s;
+    qj[0] = 2.0 * vec[0] * di[0] + vec[0] * vec[0] * s;
+    qj[1] = vec[0] * di[1] + vec[1] * di[0] + vec[0] * vec[1] * s;
+    qj[2] = 2.0 * vec[1] * di[1] + vec[1] * vec[1] * s;
+    qj[3] = vec[0] * di[2] + vec[2] * di[0] + vec[0] * vec[2] * s;
+    qj[4] = vec[1] * di[2] + vec[2] * di[1] + vec[1] * vec[2] * s;
+    qj[5] = 2.0 * vec[2] * di[2] + vec[2] * vec[2] * s;
+    traceless6(qj);
+    for (int k = 0; k < 6; k++) qj[k] += qi[k];
 }
 
 __device__ __forceinline__ double kshell(int k, int l) {
@@ -251,7 +238,7 @@ __device__ __forceinline__ void unpack_pair(long long p, int& i, int& j) {  // p
 
 // S, H0, D, Q of every atom pair (i >= j) of every molecule; m_pd0 = offsets of the pairs with
 // diagonal (sum of nat(nat+1)/2)
-__global__ void __launch_bounds__(128, 3) k_integrals(Batch B, State S, const long long* m_pd0, long long npd) {
+__global__ void k_integrals(Batch B, State S, const long long* m_pd0, long long npd) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= npd) return;
     int m = find_mol(m_pd0, B.nmol, g);
@@ -259,7 +246,7 @@ __global__ void __launch_bounds__(128, 3) k_integrals(Batch B, State S, const lo
     unpack_pair_diag(g - m_pd0[m], li, lj);
     int ia = B.m_at0[m] + li, ja = B.m_at0[m] + lj;
     int n = B.m_nao[m], ao0 = B.m_ao0[m];
-    long long mat = B.m_mat0[m];
+    long long mat = B.m_mat0[m], nn = B.nnT;
     double vec[3];
     dvec(S.xyz, ia, ja, vec);
     double r2 = vec[0] * vec[0] + vec[1] * vec[1] + vec[2] * vec[2];
@@ -267,37 +254,48 @@ __global__ void __launch_bounds__(128, 3) k_integrals(Batch B, State S, const lo
     // atom pairs beyond the conventions' distance cutoff (tblite) or screened by their exponents
     if (!onsite && (r2 > B.m_paircut2[m] || pair_screened(B.a_amin[ia], B.a_amin[ja], r2, B.intcut))) return;
     double rr = onsite ? 0.0 : sqrt(sqrt(r2) / (B.a_rad[ja] + B.a_rad[ia]));
+    double s[25], d[75], q[150];
     Shl ci, cj;
     for (int si = B.a_sh0[ia]; si < B.a_sh0[ia] + B.a_nsh[ia]; si++) {
         load_shell(B, si, ci);
         for (int sj = B.a_sh0[ja]; sj < B.a_sh0[ja] + B.a_nsh[ja]; sj++) {
             if (!onsite && pair_screened(B.s_amin[si], B.s_amin[sj], r2, B.intcut)) continue;
             load_shell(B, sj, cj);
+            multipole_block(cj, ci, vec, B.intcut, s, d, q);
             double hij;
             if (onsite) hij = 0.5 * (S.se[si] + S.se[sj]);
             else {
                 double shp = (1.0 + B.s_shpoly[si] * rr) * (1.0 + B.s_shpoly[sj] * rr);
                 hij = 0.5 * (S.se[si] + S.se[sj]) * hscale(B, sj, ja, si, ia) * shp;
             }
-            int mu0 = B.s_ao0[sj] - ao0, nu0 = B.s_ao0[si] - ao0;
-            switch (ci.l * 3 + cj.l) {
-                case 0: shell_pair_integrals<0, 0>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 1: shell_pair_integrals<0, 1>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 2: shell_pair_integrals<0, 2>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 3: shell_pair_integrals<1, 0>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 4: shell_pair_integrals<1, 1>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 5: shell_pair_integrals<1, 2>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 6: shell_pair_integrals<2, 0>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                case 7: shell_pair_integrals<2, 1>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-                default: shell_pair_integrals<2, 2>(B, S, cj, ci, vec, hij, onsite, mu0, nu0, n, mat); break;
-            }
+            int nsj = nsph(cj.l);
+            for (int im = 0; im < nsph(ci.l); im++)
+                for (int jm = 0; jm < nsj; jm++) {
+                    int k = jm + nsj * im;
+                    int mu = B.s_ao0[sj] + jm - ao0, nu = B.s_ao0[si] + im - ao0;
+                    long long e1 = mat + mu + (long long)nu * n;
+                    S.S[e1] = s[k];
+                    S.H0[e1] = s[k] * hij;
+                    for (int x = 0; x < 3; x++) S.D[x * nn + e1] = d[3 * k + x];
+                    for (int x = 0; x < 6; x++) S.Q[x * nn + e1] = q[6 * k + x];
+                    if (!onsite) {
+                        double dj[3], qj[6];
+                        shift_bra(vec, s[k], &d[3 * k], &q[6 * k], dj, qj);
+                        long long e2 = mat + nu + (long long)mu * n;
+                        S.S[e2] = s[k];
+                        S.H0[e2] = s[k] * hij;
+                        for (int x = 0; x < 3; x++) S.D[x * nn + e2] = dj[x];
+                        for (int x = 0; x < 6; x++) S.Q[x * nn + e2] = qj[x];
+                    }
+                }
         }
     }
 }
 
 // One shell pair's part of k_h0_gradient (shell si of angular momentum LI on atom i, sj of LJ on
 // atom j): compile-time sizes keep the Cartesian weights and accumulators in registers for s and p
-// shells; the operations are those of the generic loop, in the same order
+// shells; the operations of the generic loop in the same order (the compiler may fuse other
+// products: the gradient agrees to round-off)
 template <int LI, int LJ>
 __device__ __noinline__ void shell_pair_h0_gradient(const Batch& B, const State& S, const Shl& ci, const Shl& cj, int si, int sj,
                                        int ia, int ja, const double vec[3], double r2, double rr, int n, int ao0,
