@@ -459,7 +459,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         nhist += (long long)hist_span * m_dim[m];
         nsqT += (long long)h.nat * h.nat;
         long long nt = (n + 31) / 32;
-        ntiles += nt * nt;
+        ntiles += nt * (nt + 1) / 2;  // Fock tile pairs (I >= J)
         long long nw = std::max(n, 64LL);
         nwk += (axg::team_workspace((int)n) + 31) & ~31LL;
     }

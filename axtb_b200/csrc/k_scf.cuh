@@ -146,31 +146,48 @@ __device__ __forceinline__ double bterm(const Batch& B, const State& S, long lon
     return x;
 }
 
+// F = H0 - (B + B^T)/2 by pairs of 32 x 32 tiles (I, J) and (J, I), I >= J: each element's B
+// term is formed once (both tiles' B in shared memory), each matrix read once and F written once
 __global__ void k_fock(Batch B, State S, const long long* m_tile0, long long ntiles) {
-    __shared__ double bt[32][33];
+    __shared__ double ba[32][33], bb[32][33];  // ba[b][a] = B(I + a, J + b), bb[b][a] = B(J + a, I + b)
     long long tile = blockIdx.x;
     if (tile >= ntiles) return;
     int m = find_mol(m_tile0, B.nmol, tile);
     if (!mol_active(S, m)) return;
     int n = B.m_nao[m], ao0 = B.m_ao0[m];
-    int nt = (n + 31) / 32;
     long long lt = tile - m_tile0[m];
-    int ti = (int)(lt % nt), tj = (int)(lt / nt);
+    // lt = I (I + 1) / 2 + J, J <= I
+    int ti = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+    while ((long long)(ti + 1) * (ti + 2) / 2 <= lt) ti++;
+    while ((long long)ti * (ti + 1) / 2 > lt) ti--;
+    int tj = (int)(lt - (long long)ti * (ti + 1) / 2);
+    const bool diag = ti == tj;
     long long mat = B.m_mat0[m];
     int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    // transposed tile: element (J + a, I + b) for a = tx, b = ty..
     for (int b = ty; b < 32; b += 8) {
-        int row = tj * 32 + tx, col = ti * 32 + b;
-        double v = 0.0;
-        if (row < n && col < n) v = bterm(B, S, mat + row + (long long)col * n, ao0 + col);
-        bt[b][tx] = v;
+        int row = ti * 32 + tx, col = tj * 32 + b;
+        ba[b][tx] = (row < n && col < n) ? bterm(B, S, mat + row + (long long)col * n, ao0 + col) : 0.0;
+        if (!diag) {
+            int row2 = tj * 32 + tx, col2 = ti * 32 + b;
+            bb[b][tx] = (row2 < n && col2 < n) ? bterm(B, S, mat + row2 + (long long)col2 * n, ao0 + col2) : 0.0;
+        }
     }
     __syncthreads();
+    // tile (I, J): B^T from the other tile (the diagonal tile from itself)
     for (int b = ty; b < 32; b += 8) {
         int row = ti * 32 + tx, col = tj * 32 + b;
         if (row >= n || col >= n) continue;
         long long e = mat + row + (long long)col * n;
-        double f = S.H0[e] - 0.5 * (bterm(B, S, e, ao0 + col) + bt[tx][b]);
+        double f = S.H0[e] - 0.5 * (ba[b][tx] + (diag ? ba[tx][b] : bb[tx][b]));
+        if (!isfinite(f)) atomicOr(&S.status[m], ST_FOCK);
+        S.F[e] = f;
+    }
+    if (diag) return;
+    for (int b = ty; b < 32; b += 8) {
+        int row = tj * 32 + tx, col = ti * 32 + b;
+        if (row >= n || col >= n) continue;
+        long long e = mat + row + (long long)col * n;
+        double f = S.H0[e] - 0.5 * (bb[b][tx] + ba[tx][b]);
         if (!isfinite(f)) atomicOr(&S.status[m], ST_FOCK);
         S.F[e] = f;
     }
