@@ -310,7 +310,7 @@ __global__ void k_atm_pairs(Batch B, State S, const double* wt, const double* tt
             double r2bk = vbk[0] * vbk[0] + vbk[1] * vbk[1] + vbk[2] * vbk[2];
             double cralp = t6 * ta[lk] * tb[lk];
             double fdmp = 1.0 / (1.0 + cralp);
-            double ir1 = ir / (sqrt(r2ak) * sqrt(r2bk));
+            double ir1 = ir * rsqrt(r2ak * r2bk);  // 1 / (r_ab r_ak r_bk)
             double rrr2 = ir1 * ir1, rrr3 = rrr2 * ir1;
             double angf = 0.375 * rrr2 * rrr3;
             double s1 = r2ak + r2bk, d1 = (r2bk - r2ak) * (r2bk - r2ak);
