@@ -320,7 +320,7 @@ struct AxtbBatch {
     Opt opt;
     vector<HostMol> mols;
     int nmol = 0, natT = 0, nshT = 0, naoT = 0;
-    long long nnT = 0, npairT = 0, npdT = 0, nvecT = 0, nsqT = 0, ntiles = 0, nwk = 0, nhist = 0;
+    long long nnT = 0, npairT = 0, npdT = 0, nvecT = 0, nsqT = 0, ntiles = 0, nwk = 0, nhist = 0, ngamT = 0;
     int hist_cap = 0, nsp = 0;
     int mixer_kind = 0;      // the mixer plan of the run: 0 auto, 1 Broyden, 2 DIIS
     bool restart = false;    // molecules start from their previous converged moments
@@ -406,7 +406,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     for (auto& e : phase_ev) CK(cudaEventCreate(&e));
     // ---- host layout
     vector<int> m_nat(nmol), m_nsh(nmol), m_nao(nmol), m_dim(nmol);
-    vector<long long> m_hist0(nmol), m_pd0(nmol), m_tile0(nmol), m_wk0(nmol), m_sq0(nmol);
+    vector<long long> m_hist0(nmol), m_pd0(nmol), m_tile0(nmol), m_wk0(nmol), m_sq0(nmol), m_gam0(nmol);
     vector<double> m_na(nmol), m_nb(nmol), m_ch(nmol);
     m_at0.resize(nmol);
     m_sh0.resize(nmol);
@@ -427,7 +427,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     }
     const int hist_span = std::max(hist_cap, axg::DIIS_SLOTS);
     natT = nshT = naoT = 0;
-    nnT = npairT = npdT = nvecT = nsqT = ntiles = nwk = nhist = 0;
+    nnT = npairT = npdT = nvecT = nsqT = ntiles = nwk = nhist = ngamT = 0;
     for (int m = 0; m < nmol; m++) {
         HostMol& h = mols[m];
         m_nat[m] = h.nat;
@@ -443,6 +443,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         m_vec0[m] = nvecT;
         m_hist0[m] = nhist;
         m_sq0[m] = nsqT;
+        m_gam0[m] = ngamT;
         m_tile0[m] = ntiles;
         m_wk0[m] = nwk;
         m_na[m] = h.nalpha;
@@ -458,6 +459,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
         nvecT += m_dim[m];
         nhist += (long long)hist_span * m_dim[m];
         nsqT += (long long)h.nat * h.nat;
+        ngamT += (long long)h.nsh * h.nsh;
         long long nt = (n + 31) / 32;
         ntiles += nt * (nt + 1) / 2;  // Fock tile pairs (I >= J)
         long long nw = std::max(n, 64LL);
@@ -673,6 +675,8 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     auto addL = [&](size_t n) { bytes += padded<long long>(n); };
     addI(nmol * 7);
     addL(nmol * 10);
+    addL(nmol);                                    // shell gamma matrix offsets
+    addD((size_t)std::max(ngamT, 1LL));           // shell gamma matrices
     addD(nmol * 3);
     addD(nmol);  // per-molecule pair cutoffs
     addI(natT * 6);
@@ -760,6 +764,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     b.m_ao0 = upI(m_ao0);
     b.m_dim = upI(m_dim);
     b.m_mat0 = upL(m_mat0);
+    b.m_gam0 = upL(m_gam0);
     b.m_vec0 = upL(m_vec0);
     b.m_pair0 = upL(m_pair0);
     d_pair0 = const_cast<long long*>(b.m_pair0);
@@ -1071,6 +1076,7 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     }
     s.red = ar.take<double>((size_t)axg::team_red_doubles(grid));  // grid-team partials
     s.eeq_A = ar.take<double>((size_t)nsqT * 3);
+    s.gam = ar.take<double>((size_t)std::max(ngamT, 1LL));
     // team plan
     P.big = upI(big);
     P.nbig = (int)big.size();
@@ -1353,6 +1359,7 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     CK(cudaMemsetAsync(S.ts, 0, sizeof(double) * nmol, st));
     // geometry
     LAUNCH("cn", 0, 0, k_cn<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
+    if (ngamT > 0) LAUNCH("gamma", 0, 0, k_gamma<<<blocks_for(ngamT, T), T, 0, st>>>(B, S, ngamT));
     LAUNCH("selfenergy", 0, 0, k_selfenergy<<<blocks_for(std::max(natT, nshT), T), T, 0, st>>>(B, S));
     LAUNCH("repulsion", 0, 0, k_repulsion<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));
     LAUNCH("mol_sum", 0, 0, k_mol_sum<<<nmol, T, 0, st>>>(B, S.e_atom, S.e_fixed));

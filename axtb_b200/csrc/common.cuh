@@ -39,6 +39,7 @@ struct Batch {
     // molecules
     const int *m_nat, *m_nsh, *m_nao, *m_at0, *m_sh0, *m_ao0, *m_dim;
     const long long *m_mat0, *m_vec0, *m_pair0, *m_hist0;
+    const long long* m_gam0;          // per-molecule offsets of the shell gamma matrices (sum nsh^2)
     const double *m_nalpha, *m_nbeta, *m_charge;
     // atoms
     const int *a_Z, *a_mol, *a_sh0, *a_nsh, *a_ao0, *a_sp;
@@ -137,6 +138,7 @@ struct State {
     // cooperative scratch
     double* red;       // reduction partials (grid-size * 8)
     double* eeq_A;     // EEQ system matrices (sum (nat)^2)
+    double* gam;       // shell gamma matrices of the geometry, per molecule nsh x nsh (row s, column t)
     long long* m_eeq0;
 };
 

@@ -27,6 +27,18 @@ __device__ __forceinline__ double gamma_el(const Batch& B, const double* x, int 
     return 1.0 / sqrt(r2 + 1.0 / (eta * eta));
 }
 
+// the shell gamma matrix of each molecule's geometry (crates/axtb/src/coulomb.rs:61-119), made once
+// per run and read by every SCC iteration's potentials and energies: thread per element
+__global__ void k_gamma(Batch B, State S, long long ngam) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngam) return;
+    int m = find_mol(B.m_gam0, B.nmol, g);
+    int nsh = B.m_nsh[m], sh0 = B.m_sh0[m];
+    long long l = g - B.m_gam0[m];
+    int s = (int)(l / nsh), t = (int)(l - (long long)s * nsh);
+    S.gam[g] = gamma_el(B, S.xyz, sh0 + s, sh0 + t);
+}
+
 // AES pair factors g3 = f3/r^3, g5 = f5/r^5 (crates/axtb/src/coulomb.rs:382-394)
 __device__ __forceinline__ void aes_g35(const State& S, int a, int b, double r2, double& g3, double& g5) {
     double r1 = sqrt(r2), g1 = 1.0 / r1;
@@ -72,7 +84,8 @@ __global__ void k_potentials(Batch B, State S) {
     // ES2 + ES3 for the shells of atom a
     for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
         double v = 0.0;
-        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gamma_el(B, x, s, t) * S.qsh_in[t];
+        const double* gs = S.gam + B.m_gam0[mv.m] + (long long)(s - sh0) * nsh - sh0;
+        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gs[t] * S.qsh_in[t];
         v = warp_sum(v);
         if (lane == 0) S.vsh[s] = v + S.qsh_in[s] * S.qsh_in[s] * B.s_gam3[s];
     }
@@ -256,7 +269,8 @@ __global__ void k_energy(Batch B, State S) {
     double e = 0.0, e2 = 0.0, e3 = 0.0, eaes = 0.0, ed = 0.0;
     for (int s = B.a_sh0[a]; s < B.a_sh0[a] + B.a_nsh[a]; s++) {
         double v = 0.0;
-        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gamma_el(B, x, s, t) * S.qsh_out[t];
+        const double* gs = S.gam + B.m_gam0[mv.m] + (long long)(s - sh0) * nsh - sh0;
+        for (int t = sh0 + lane; t < sh0 + nsh; t += 32) v += gs[t] * S.qsh_out[t];
         v = warp_sum(v);
         double q = S.qsh_out[s];
         e2 += 0.5 * q * v;
