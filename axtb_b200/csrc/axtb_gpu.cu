@@ -620,7 +620,15 @@ void AxtbBatch::build(const vector<HostMol>& in, const Opt& o) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
     int per = 0;
     CK(cudaFuncSetAttribute((const void*)axg::k_team, cudaFuncAttributeMaxDynamicSharedMemorySize, axg::SMEM_WORK_BYTES));
+    CK(cudaFuncSetAttribute((const void*)axg::k_team_grid, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            axg::SMEM_WORK_BYTES));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, axg::k_team, axg::TEAM_THREADS, axg::SMEM_WORK_BYTES));
+    {
+        int per_grid = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_grid, axg::k_team_grid, axg::TEAM_THREADS,
+                                                         axg::SMEM_WORK_BYTES));
+        per = std::min(per, per_grid);
+    }
     if (per <= 0) throw Fail(AXTB_ERR_DEVICE, "team kernel does not fit on a multiprocessor");
     grid = nsm * std::min(per, 2);
     vector<int> big, small_off(grid + 1, 0), small_list, head_off, head_list, tail_off, tail_list;
@@ -1391,19 +1399,32 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
     void* args[] = {&B, &S, &P, nullptr};
     int ph = PH_OVERLAP;
     args[3] = &ph;
+    // a team phase: the whole-grid molecules in their own launch (k_team_grid), then the rest
+    TeamPlan Psmall = P;
+    Psmall.nbig = 0;
+    void* args_small[] = {&B, &S, &Psmall, &ph};
+    auto team_launch = [&](int phase) {
+        ph = phase;
+        Psmall = P;
+        Psmall.nbig = 0;
+        if (P.nbig > 0 && phase != PH_EIGEN_TAIL) {  // no whole-grid molecule has a part after k_chase
+            CK(cudaLaunchCooperativeKernel((void*)k_team_grid, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st));
+            launches++;
+        }
+        CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args_small, SMEM_WORK_BYTES, st));
+    };
     double chol_flops = 0.0;
     for (int m = 0; m < nmol; m++) chol_flops += (1.0 / 3.0 + 2.0 / 3.0) * std::pow((double)mols[m].nao, 3.0);
     LAUNCH("team_overlap", chol_flops, 0,
-           CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
+           team_launch(PH_OVERLAP));
     bool eeq = opt.guess == 0 && eeq_guess && !warm;
     if (warm) {
         LAUNCH("start", 0, 0, k_start_warm<<<nmol, T, 0, st>>>(B, S, mixer_kind, nullptr));
     } else if (eeq) {
         LAUNCH("eeq_matrix", 0, 0, k_eeq_matrix<<<blocks_for(nsqT, T), T, 0, st>>>(B, S, d_sq0, P.eeq_rhs, nsqT));
-        ph = PH_EEQ;
         double f = 0.0;
         for (int m = 0; m < nmol; m++) f += 3.0 * std::pow((double)mols[m].nat, 3.0);
-        LAUNCH("team_eeq", f, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
+        LAUNCH("team_eeq", f, 0, team_launch(PH_EEQ));
     }
     if (!warm) LAUNCH("start", 0, 0, k_start<<<nmol, T, 0, st>>>(B, S, P.eeq_q, eeq ? 1 : 0, mixer_kind, nullptr));
     // restarts: a molecule with converged moments from the previous run starts from them
@@ -1420,14 +1441,12 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
             LAUNCH("fock", 0, mat_bytes(act, 12.0), k_fock<<<(unsigned)ntiles, T, 0, st>>>(B, S, d_tile0, ntiles));
             // the eigen phase: one launch, or three when k_chase takes stage 2 of some molecules
             LAUNCH("team_eigen", eig_flops(act), 0, {
-                ph = PH_EIGEN;
-                CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st));
+                team_launch(PH_EIGEN);
                 if (nchase > 0) {
                     CP.cycles = P.cycles;
                     k_chase<<<chase_grid, CHASE_THREADS, CHASE_DYN_BYTES, st>>>(B, S, CP);
                     CK(cudaGetLastError());
-                    ph = PH_EIGEN_TAIL;
-                    CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st));
+                    team_launch(PH_EIGEN_TAIL);
                     launches += 2;
                 }
             });
@@ -1486,14 +1505,11 @@ void AxtbBatch::run(bool want_grad, bool warm, bool want_levels) {
         CK(cudaMemcpyAsync(S.have_guess, S.conv, sizeof(int) * nmol, cudaMemcpyDeviceToDevice, st));
     }
     if (want_levels) {
-        ph = PH_LEVELS;
-        LAUNCH("team_levels", 0, 0, CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
+        LAUNCH("team_levels", 0, 0, team_launch(PH_LEVELS));
     }
     CK(cudaEventRecord(phase_ev[2], st));
     if (want_grad) {
-        ph = PH_WDENS;
-        LAUNCH("team_wdens", w_flops(all), 0,
-               CK(cudaLaunchCooperativeKernel((void*)k_team, grid, TEAM_THREADS, args, SMEM_WORK_BYTES, st)));
+        LAUNCH("team_wdens", w_flops(all), 0, team_launch(PH_WDENS));
         if (B.output_aes)
             LAUNCH("gradient_potentials", 0, 0,
                    k_gradient_potentials_aes<<<blocks_for((long long)natT * 32, T), T, 0, st>>>(B, S));

@@ -155,6 +155,9 @@ __device__ __forceinline__ bool chased_on_chip(const Team& t, const Batch& B, in
 
 // after_chase: the part after k_chase of a molecule whose bulge chasing ran on chip (from its
 // tridiagonal matrix on); otherwise the whole eigen phase, or for such a molecule the part before
+// GRID_ROWS: the whole-grid instance (k_team_grid), whose tridiagonal reduction sums the symv rows
+// warp by warp (grid_symv_combine); k_team and the allocation-free entry point use the other
+template <bool GRID_ROWS = false>
 __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPlan& P, int m, bool after_chase) {
     int n = B.m_nao[m], ao0 = B.m_ao0[m];
     long long mat = B.m_mat0[m];
@@ -196,8 +199,8 @@ __device__ void mol_eigen(const Team& t, const Batch& B, State& S, const TeamPla
         TEAM_PHASE(17);
     } else {
         double* Vp = wk + 2 * n + (long long)nsl * n;  // the back-transform's vb area (64 n)
-        team_tridiag_blocked(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
-                             P.cycles != 0);
+        team_tridiag_blocked<GRID_ROWS>(t, Fp, n, n, d, e, tau, Vp, Vp + (long long)NBP * n, vbuf, pbuf, ppart, S.red,
+                                        P.cycles != 0);
         if (P.cycles && t.tid() == 0) t0__ = clock64();  // the tridiagonal's parts were counted in 8..13
     }
     TEAM_PHASE(1);
@@ -297,13 +300,14 @@ __device__ __forceinline__ bool phase_wants(const State& S, int phase, int m) {
     return true;
 }
 
+template <bool GRID_ROWS>
 __device__ void run_mol(const Team& t, const Batch& B, State& S, const TeamPlan& P, int phase, int m) {
     switch (phase) {
         case PH_OVERLAP: mol_overlap(t, B, S, P, m); break;
         case PH_EEQ: mol_eeq(t, B, S, P, m); break;
         case PH_EIGEN:
         case PH_EIGEN_TAIL:
-            if (phase == PH_EIGEN || chased_on_chip(t, B, B.m_nao[m])) mol_eigen(t, B, S, P, m, phase == PH_EIGEN_TAIL);
+            if (phase == PH_EIGEN || chased_on_chip(t, B, B.m_nao[m])) mol_eigen<GRID_ROWS>(t, B, S, P, m, phase == PH_EIGEN_TAIL);
             break;
         case PH_WDENS: mol_wdens(t, B, S, P, m); break;
         case PH_LEVELS: mol_levels(t, B, S, P, m); break;
@@ -316,14 +320,28 @@ __global__ void __launch_bounds__(TEAM_THREADS, 2) k_team(Batch B, State S, Team
     Team g{(int)blockIdx.x, (int)gridDim.x, true};
     for (int i = 0; i < P.nbig; i++) {
         int m = P.big[i];
-        if (phase_wants(S, phase, m)) run_mol(g, B, S, P, phase, m);  // uniform across the grid
+        if (phase_wants(S, phase, m)) run_mol<false>(g, B, S, P, phase, m);  // uniform across the grid
     }
     Team one{0, 1, false};
     const int* off = phase == PH_EIGEN ? P.head_off : phase == PH_EIGEN_TAIL ? P.tail_off : P.small_off;
     const int* list = phase == PH_EIGEN ? P.head_list : phase == PH_EIGEN_TAIL ? P.tail_list : P.small_list;
     for (int i = off[blockIdx.x]; i < off[blockIdx.x + 1]; i++) {
         int m = list[i];
-        if (phase_wants(S, phase, m)) run_mol(one, B, S, P, phase, m);
+        if (phase_wants(S, phase, m)) run_mol<false>(one, B, S, P, phase, m);
+    }
+}
+
+// The whole-grid molecules (P.big) of a phase, one after the other on the whole cooperative grid.
+// A batch that holds such molecules runs this launch first and then k_team for the rest (with
+// nbig = 0): the grid path gets its own instance of the dense algebra, and the one-CTA path's
+// kernel is compiled without the grid-only code.
+__global__ void __launch_bounds__(TEAM_THREADS, 2) k_team_grid(Batch B, State S, TeamPlan P, int phase) {
+    if (threadIdx.x == 0) s_team_gen = 0;
+    __syncthreads();
+    Team g{(int)blockIdx.x, (int)gridDim.x, true};
+    for (int i = 0; i < P.nbig; i++) {
+        int m = P.big[i];
+        if (phase_wants(S, phase, m)) run_mol<true>(g, B, S, P, phase, m);  // uniform across the grid
     }
 }
 

@@ -676,6 +676,46 @@ __device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long
     return rt;
 }
 
+// Grid team: the rows' symv sums, p_i = tau (sum of row i's slots - W_i. ys[0:c] - V_i. ys[c:2c]),
+// into pbuf; returns this thread's part of p . v. A warp per row (rows spread over the whole
+// grid), lanes over the row's slots with all of a lane's loads in flight at once, then lanes over
+// the panel's c terms, with butterfly sums in a fixed order. (A one-CTA team sums each row in one
+// thread, four slots at a time; for a large matrix that left the last row blocks, with hundreds
+// of slots each, to a few CTAs while the rest of the grid waited.)
+__device__ __noinline__ double grid_symv_combine(const Team& t, const double* ppart, int rt, int r0, int n,
+                                                 const double* V, const double* W, long long ldv, const double* ys,
+                                                 int c, double tj, const double* vbuf, double* pbuf) {
+    int lane = threadIdx.x & 31;
+    double pv = 0.0;
+    for (int i = r0 + t.warp(); i < n; i += t.nwarps()) {
+        int nsl = 3 * ((i - r0) >> 6) + 4 + rt;
+        const double* pp = ppart + i;
+        double s = 0.0;
+        for (int k0 = 0; k0 < nsl; k0 += 256) {
+            double x[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                int k = k0 + u * 32 + lane;
+                x[u] = k < nsl ? __ldcg(pp + (long long)k * n) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) s += x[u];
+        }
+        double wv = 0.0;
+        if (lane < c) wv = W[i + lane * ldv] * ys[lane] + V[i + lane * ldv] * ys[c + lane];
+        s = (warp_sum(s) - warp_sum(wv)) * tj;
+        if (lane == 0) {
+            pbuf[i] = s;
+            pv += s * vbuf[i];
+        }
+    }
+    return pv;
+}
+
+// GRID_ROWS: the instance for whole-grid teams (t.global), with the row sums of
+// grid_symv_combine; the one-CTA instance is compiled without that code, so the batch path's
+// hot loop keeps its own register allocation.
+template <bool GRID_ROWS>
 __device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long long lda, int n, double* d, double* e, double* tau,
                                      double* V, double* W, double* vbuf, double* pbuf, double* ppart, double* gred,
                                      bool cyc = false) {
@@ -744,28 +784,35 @@ __device__ __noinline__ void team_tridiag_blocked(const Team& t, double* A, long
                 team_panel_dots(t, V, W, ldv, vbuf, r0, n, c, ys, gred);  // its barrier also publishes ppart
                 tick(11);
                 double pv = 0.0;
-                for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
-                    int nsl = 3 * ((i - r0) >> 6) + 4 + rt;  // this row's symv slots
-                    // four independent partial sums (four loads in flight), combined in a fixed order
-                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-                    const double* pp = ppart + i;
-                    int ch = 0;
-                    for (; ch + 3 < nsl; ch += 4) {
-                        s0 += pp[(long long)ch * n];
-                        s1 += pp[(long long)(ch + 1) * n];
-                        s2 += pp[(long long)(ch + 2) * n];
-                        s3 += pp[(long long)(ch + 3) * n];
+                bool grid_rows = false;
+                if constexpr (GRID_ROWS) grid_rows = t.global;
+                if (grid_rows) {
+                    pv = grid_symv_combine(t, ppart, rt, r0, n, V, W, ldv, ys, c, tj, vbuf, pbuf);
+                } else {
+                    for (int i = r0 + t.tid(); i < n; i += t.nthreads()) {
+                        int nsl = 3 * ((i - r0) >> 6) + 4 + rt;  // this row's symv slots
+                        // four independent partial sums (four loads in flight), combined in a fixed order
+                        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                        const double* pp = ppart + i;
+                        int ch = 0;
+                        for (; ch + 3 < nsl; ch += 4) {
+                            s0 += pp[(long long)ch * n];
+                            s1 += pp[(long long)(ch + 1) * n];
+                            s2 += pp[(long long)(ch + 2) * n];
+                            s3 += pp[(long long)(ch + 3) * n];
+                        }
+                        for (; ch < nsl; ch++) s0 += pp[(long long)ch * n];
+                        double s = (s0 + s1) + (s2 + s3);
+                        for (int q = 0; q < c; q++) s -= W[i + q * ldv] * ys[q] + V[i + q * ldv] * ys[c + q];
+                        s *= tj;
+                        pbuf[i] = s;
+                        pv += s * vbuf[i];
                     }
-                    for (; ch < nsl; ch++) s0 += pp[(long long)ch * n];
-                    double s = (s0 + s1) + (s2 + s3);
-                    for (int q = 0; q < c; q++) s -= W[i + q * ldv] * ys[q] + V[i + q * ldv] * ys[c + q];
-                    s *= tj;
-                    pbuf[i] = s;
-                    pv += s * vbuf[i];
                 }
                 double dot = team_sum(t, pv, gred);
                 double K = -0.5 * tj * dot;
-                for (int i = r0 + t.tid(); i < n; i += t.nthreads()) W[i + c * ldv] = pbuf[i] + K * vbuf[i];
+                for (int i = r0 + t.tid(); i < n; i += t.nthreads())
+                    W[i + c * ldv] = (grid_rows ? __ldcg(pbuf + i) : pbuf[i]) + K * vbuf[i];
             } else {
                 for (int i = r0 + t.tid(); i < n; i += t.nthreads()) W[i + c * ldv] = 0.0;
             }
