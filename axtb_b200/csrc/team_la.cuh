@@ -678,35 +678,55 @@ __device__ __noinline__ int team_symv_lower(const Team& t, const double* A, long
 
 // Grid team: the rows' symv sums, p_i = tau (sum of row i's slots - W_i. ys[0:c] - V_i. ys[c:2c]),
 // into pbuf; returns this thread's part of p . v. A warp per row (rows spread over the whole
-// grid), lanes over the row's slots with all of a lane's loads in flight at once, then lanes over
-// the panel's c terms, with butterfly sums in a fixed order. (A one-CTA team sums each row in one
-// thread, four slots at a time; for a large matrix that left the last row blocks, with hundreds
-// of slots each, to a few CTAs while the rest of the grid waited.)
+// grid), lanes over the row's slots, then lanes over the panel's c terms, with butterfly sums in
+// a fixed order; a warp's rows (i, i + nwarps, i + 2 nwarps) are taken three at a time with all
+// of their loads in flight together. (A one-CTA team sums each row in one thread, four slots at a
+// time; for a large matrix that left the last row blocks, with hundreds of slots each, to a few
+// CTAs while the rest of the grid waited.)
 __device__ __noinline__ double grid_symv_combine(const Team& t, const double* ppart, int rt, int r0, int n,
                                                  const double* V, const double* W, long long ldv, const double* ys,
                                                  int c, double tj, const double* vbuf, double* pbuf) {
+    constexpr int R = 3;
     int lane = threadIdx.x & 31;
+    int nw = t.nwarps();
     double pv = 0.0;
-    for (int i = r0 + t.warp(); i < n; i += t.nwarps()) {
-        int nsl = 3 * ((i - r0) >> 6) + 4 + rt;
-        const double* pp = ppart + i;
-        double s = 0.0;
-        for (int k0 = 0; k0 < nsl; k0 += 256) {
-            double x[8];
+    for (int i0 = r0 + t.warp(); i0 < n; i0 += R * nw) {
+        int nsl[R];
+        double s[R], wv[R];
+        int nmax = 0;
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
-                int k = k0 + u * 32 + lane;
-                x[u] = k < nsl ? __ldcg(pp + (long long)k * n) : 0.0;
+        for (int r = 0; r < R; r++) {
+            int i = i0 + r * nw;
+            nsl[r] = i < n ? 3 * ((i - r0) >> 6) + 4 + rt : 0;
+            nmax = max(nmax, nsl[r]);
+            s[r] = 0.0;
+            wv[r] = 0.0;
+            if (i < n && lane < c) wv[r] = W[i + lane * ldv] * ys[lane] + V[i + lane * ldv] * ys[c + lane];
+        }
+        for (int k0 = 0; k0 < nmax; k0 += 256) {
+            double x[R][8];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const double* pp = ppart + (i0 + r * nw);
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    int k = k0 + u * 32 + lane;
+                    x[r][u] = k < nsl[r] ? __ldcg(pp + (long long)k * n) : 0.0;
+                }
             }
 #pragma unroll
-            for (int u = 0; u < 8; u++) s += x[u];
+            for (int r = 0; r < R; r++)
+#pragma unroll
+                for (int u = 0; u < 8; u++) s[r] += x[r][u];
         }
-        double wv = 0.0;
-        if (lane < c) wv = W[i + lane * ldv] * ys[lane] + V[i + lane * ldv] * ys[c + lane];
-        s = (warp_sum(s) - warp_sum(wv)) * tj;
-        if (lane == 0) {
-            pbuf[i] = s;
-            pv += s * vbuf[i];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            int i = i0 + r * nw;
+            double sr = (warp_sum(s[r]) - warp_sum(wv[r])) * tj;
+            if (lane == 0 && i < n) {
+                pbuf[i] = sr;
+                pv += sr * vbuf[i];
+            }
         }
     }
     return pv;
